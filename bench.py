@@ -1,0 +1,372 @@
+#!/usr/bin/env python3
+"""Benchmark of the p2r hot path on B200: track-layer updates/s of the fused chained forward.
+
+Workload (one "step"): the fused forward (propagateToR + KalmanUpdate for every layer of
+every track, chained) over 9600 tracks x 100 events x 20 layers, bsize 32, Bz 3.8 T,
+synthetic helices (p2r_gen_helix). Inputs (0.80 GB) exceed the 126 MB L2, so no flush is
+needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank runs its own events (weak scaling, no data-path
+collective: tracks are independent); the timed region is bracketed by barriers and device
+synchronisation and the max over ranks is taken. Rank 0 prints one JSON line.
+
+--impl reference times the reference's own CPU path (src/propagate-tor-test_tbb.cpp,
+compiled unmodified into oracle/_ref/) on all host threads, on the same metric and workload
+(each step a bounded sample of its events).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "track-layer updates/s at 960k trk×20 lyr FP32; fwd+adjoint time vs plain fwd"
+FLOP_PER_UPDATE = 1272  # 958 propagateToR + 314 KalmanUpdate FP32 ops (FMA = 2)
+FP64_OPS_PER_UPDATE = 4
+NTRKS, NEVTS, NLAYER, BSIZE, BZ = 9600, 100, 20, 32, 3.8
+NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4 at the 1965 MHz max SM clock
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--bsize", type=int, default=BSIZE)
+    ap.add_argument("--nevts", type=int, default=NEVTS)
+    ap.add_argument("--mode", choices=["chained", "restart"], default="chained")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--ref-budget", type=float, default=90.0, help="reference arm: total seconds")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ workload
+def make_inputs(p2r, nevts, bsize, seed):
+    cfg = p2r.Config(bsize=bsize, nlayer=NLAYER, nevts=nevts, nb=NTRKS // bsize, bz=BZ,
+                     mode=p2r.MODE_CHAINED)
+    trk, hit = p2r.generate_helix(cfg, p2r.gen_params(bz=BZ, seed=seed))
+    return cfg, trk, hit
+
+
+def traffic_from_profiles(workload_key: str):
+    """Per-launch DRAM bytes of the fused kernel from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "fwd_kernel_chained_9600x100x20.md"
+    if not f.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+def measured_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return json.loads(f.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+# ------------------------------------------------------------------ CPU reference timing
+def cpu_reference_rate(trk, hit, nevts, nb, bsize, budget_s, nthreads):
+    """Times the reference's own driver loop (oracle/_ref) on a bounded sample of events.
+    Returns (updates/s, sample description, kind, threads)."""
+    from oracle.oracle import RefTBB, ref_available, host_isa
+    kind = host_isa()
+    if not ref_available(bsize, kind):
+        raise RuntimeError("reference CPU build (oracle/_ref) is missing")
+    ref = RefTBB(bsize, kind)
+    tw = 28 * bsize * nb  # floats per event of tracks
+    hw = 9 * bsize * nb * NLAYER
+    # probe one event to size the sample
+    t0 = time.perf_counter()
+    ref.run_into(trk[:tw], hit[:hw], np.empty(tw, np.float32), 1, nb, NLAYER, True, 1, nthreads)
+    t_ev = max(time.perf_counter() - t0, 1e-4)
+    nev = int(min(nevts, max(1, budget_s / 3 / t_ev)))
+    out = np.empty(nev * tw, np.float32)
+    reps, done, t_tot = 0, 0, 0.0
+    while t_tot < budget_s / 2 or reps == 0:
+        t0 = time.perf_counter()
+        ref.run_into(trk[: nev * tw], hit[: nev * hw], out, nev, nb, NLAYER, True, 1, nthreads)
+        t_tot += time.perf_counter() - t0
+        reps += 1
+        done += nev * nb * bsize * NLAYER
+        if reps >= 1000:
+            break
+    sample = (f"{reps} pass(es) of the chained reference loop over {nev} of {nevts} events "
+              f"({nev * nb * bsize} tracks x {NLAYER} layers), {t_tot:.1f} s wall")
+    return done / t_tot, sample, kind, nthreads
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import p2r_tests_b200 as p2r
+    nthreads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    from oracle.oracle import ref_available, host_isa
+    if not ref_available(args.bsize, host_isa()):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref missing"}))
+        return 0
+    nb = NTRKS // args.bsize
+    cfg, trk, hit = make_inputs(p2r, args.nevts, args.bsize, 20240001)
+    trk, hit = trk.reshape(-1), hit.reshape(-1)
+    from oracle.oracle import RefTBB
+    ref = RefTBB(args.bsize, host_isa())
+    tw, hw = 28 * args.bsize * nb, 9 * args.bsize * nb * NLAYER
+    t0 = time.perf_counter()
+    ref.run_into(trk[:tw], hit[:hw], np.empty(tw, np.float32), 1, nb, NLAYER, True, 1, nthreads)
+    t_ev = max(time.perf_counter() - t0, 1e-4)
+    per_step = args.ref_budget / max(1, args.steps + args.warmup)
+    nev = int(min(args.nevts, max(1, per_step / t_ev)))
+    out = np.empty(nev * tw, np.float32)
+    for _ in range(args.warmup):
+        ref.run_into(trk[: nev * tw], hit[: nev * hw], out, nev, nb, NLAYER, True, 1, nthreads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.run_into(trk[: nev * tw], hit[: nev * hw], out, nev, nb, NLAYER, True, 1, nthreads)
+        times.append(time.perf_counter() - t0)
+    ups = nev * nb * args.bsize * NLAYER
+    tot = sum(times)
+    value = ups * len(times) / tot
+    sample = f"{nev} of {args.nevts} events per step ({nev * nb * args.bsize} tracks x {NLAYER} layers, chained)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "track-layer updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": "track-layer updates/s", "cores": nthreads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "track-layer updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def workload_config(args):
+    return {"workload": f"fused {args.mode} p2r forward (propagateToR + KalmanUpdate per layer), "
+                        f"{NTRKS} tracks x {args.nevts} events x {NLAYER} layers per GPU",
+            "ntrks": NTRKS, "nevts": args.nevts, "nlayer": NLAYER, "bsize": args.bsize, "bz_tesla": BZ,
+            "mode": args.mode, "generator": "p2r_gen_helix defaults (seeded synthetic helices)",
+            "l2": "inputs (0.80 GB per GPU) larger than the 126 MB L2; no flush"}
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import p2r_tests_b200 as p2r
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    cfg, trk, hit = make_inputs(p2r, args.nevts, args.bsize, 20240001 + rank)
+    cfg.mode = p2r.MODE_CHAINED if args.mode == "chained" else p2r.MODE_RESTART
+    d_trk = torch.from_numpy(trk.reshape(-1)).to(dev)
+    d_hit = torch.from_numpy(hit.reshape(-1)).to(dev)
+    d_out = torch.empty_like(d_trk)
+    stream = torch.cuda.current_stream(dev)
+    updates = cfg.ntracks * NLAYER  # per step per GPU (restart counts the same work unit)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    for _ in range(max(3, args.warmup)):
+        p2r.forward(cfg, d_trk, d_hit, d_out, stream=stream)
+    torch.cuda.synchronize()
+
+    # timed region: exactly K steps of the fused kernel
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.2)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        p2r.forward(cfg, d_trk, d_hit, d_out, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    t_ms = max_over_ranks(e0.elapsed_time(e1))
+    ms_per_step = t_ms / args.steps
+    value = world * updates * args.steps / (t_ms / 1e3)
+    nonfinite = p2r.count_nonfinite(d_out, cfg.nblocks, cfg.bsize)
+
+    # roofline of the fused kernel (the only kernel of a step): FP32 compute
+    t_launch = ms_per_step / 1e3
+    flops = FLOP_PER_UPDATE * updates
+    achieved_tflops = flops / t_launch / 1e12
+    probe_out = torch.empty(148 * 8 * 256, dtype=torch.float32, device=dev)
+    p2r.fp32_fma_probe(probe_out, 2000, 148 * 8, 256, stream=stream)
+    torch.cuda.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record(stream)
+    pflops = 0
+    for _ in range(5):
+        pflops += p2r.fp32_fma_probe(probe_out, 20000, 148 * 8, 256, stream=stream)
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    fp32_peak = pflops / (pe0.elapsed_time(pe1) / 1e3) / 1e12
+    alg_bytes = cfg.ntracks * (36 * NLAYER + 224)
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs")
+    traffic = traffic_from_profiles("chained")
+
+    # end to end through the host-buffer C-ABI call: H2D + kernels + D2H every step
+    h_trk = torch.from_numpy(trk.reshape(-1)).pin_memory().numpy()
+    h_hit = torch.from_numpy(hit.reshape(-1)).pin_memory().numpy()
+    h_out = torch.empty(trk.size, dtype=torch.float32).pin_memory().numpy()
+    for _ in range(2):
+        p2r.forward_host(cfg, h_trk, h_hit, h_out, d_trk, d_hit, d_out, nchunks=10, stream=stream)
+    torch.cuda.synchronize()
+    barrier()
+    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    for _ in range(args.e2e_steps):
+        p2r.forward_host(cfg, h_trk, h_hit, h_out, d_trk, d_hit, d_out, nchunks=10, stream=stream)
+    x1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(x0.elapsed_time(x1))
+    e2e_value = world * updates * args.e2e_steps / (e2e_ms / 1e3)
+    ok = np.array_equal(h_out.view(np.uint32), d_out.cpu().numpy().view(np.uint32))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            nthreads = len(os.sched_getaffinity(0))
+            v, sample, kind, thr = cpu_reference_rate(trk.reshape(-1), hit.reshape(-1), args.nevts, cfg.nb,
+                                                      cfg.bsize, args.cpu_seconds, nthreads)
+            cpu = {"value": v, "unit": "track-layer updates/s", "cores": thr, "kind": "reference",
+                   "sample": sample + f"; reference build oracle/_ref ({kind}), Bz compiled in at 3.8112 T"}
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": "track-layer updates/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "track-layer updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args),
+            "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved_tflops / fp32_peak,
+                         "traffic": traffic,
+                         "peak_source": "measured in this run: p2r_fp32_fma_probe (FP32 FMA, full occupancy); "
+                                        f"nominal {NOMINAL_FP32_TFLOPS:.1f} at 1965 MHz",
+                         "frac_of_nominal": achieved_tflops / NOMINAL_FP32_TFLOPS,
+                         "flop_per_update": FLOP_PER_UPDATE, "updates_per_launch": updates,
+                         "launch_ms": ms_per_step},
+            "roofline_hbm": {"bound": "hbm", "achieved": alg_bytes / t_launch / 1e9,
+                             "peak": hbm_peak, "unit": "GB/s",
+                             "frac": (alg_bytes / t_launch / 1e9 / hbm_peak) if hbm_peak else None,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                             "algorithmic_bytes_per_launch": alg_bytes},
+            "e2e": {"value": e2e_value, "unit": "track-layer updates/s",
+                    "h2d_bytes_per_step": int(trk.nbytes + hit.nbytes), "d2h_bytes_per_step": int(trk.nbytes),
+                    "steps": args.e2e_steps, "api": "p2r_forward_host (pinned host buffers, 10 chunks)",
+                    "output_matches_device_run": bool(ok)},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "nonfinite_tracks": nonfinite,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+        sys.stdout.flush()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,196 @@
+/*
+ * p2r-b200: C ABI of the B200-native (sm_100a) track-propagation and Kalman-update path.
+ *
+ * Reference: cerati/p2r-tests, src/propagate-tor-test_tbb.cpp ("TBB" below). The
+ * reference has no library interface: its per-block functions propagateToR (TBB:656-657)
+ * and KalmanUpdate (TBB:433) are called by a driver loop (TBB:870-926) over caller-owned
+ * Matriplex arrays. This header exposes the same arithmetic over the same arrays.
+ *
+ * Data layout (identical to the reference's structs, TBB:56-125, with bsize a run-time
+ * value instead of a macro):
+ *   MPTRK block = { float par[6*bsize]; float cov[21*bsize]; int32 q[bsize]; }  112*bsize B
+ *   MPHIT block = { float pos[3*bsize]; float cov[6*bsize]; }                    36*bsize B
+ *   element (lane it, component ip) of a block is data[it + ip*bsize].
+ *   par = (x, y, z, 1/pT, phi, theta); symmetric matrices are packed lower-triangle
+ *   row-major, (i >= j) -> i*(i+1)/2 + j (TBB:46-54).
+ *   Track block of event ev, block ib:  tracks[ib + nb*ev]                (TBB:147-153)
+ *   Hit block of layer lay:             hits[lay + ib*nlayer + ev*nlayer*nb] (TBB:215-217)
+ *
+ * Conventions: every pointer is a device pointer unless its name starts with host_;
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream); calls are
+ * asynchronous and stream-ordered; nothing allocates device memory except where a
+ * function says so. Every function returns a p2r_status; p2r_last_error_string() gives
+ * the message of the calling thread's last failure. No function aborts the process
+ * (the reference aborts on CUDA errors, include/cudaCheck.h:17-58).
+ */
+#ifndef P2R_B200_H
+#define P2R_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define P2R_ABI_VERSION 1
+
+typedef enum p2r_status {
+  P2R_OK = 0,
+  P2R_ERR_INVALID = 1,     /* bad argument: null pointer, size, alignment, mode */
+  P2R_ERR_CUDA = 2,        /* a CUDA runtime call failed (message has the CUDA error) */
+  P2R_ERR_TIMEOUT = 3,     /* a bounded device-side wait ran out */
+  P2R_ERR_UNSUPPORTED = 4, /* valid request this build does not implement */
+  P2R_ERR_WORKSPACE = 5,   /* workspace missing or too small */
+  P2R_ERR_QUEUE = 6        /* malformed work-queue description */
+} p2r_status;
+
+/* Layer-loop semantics (both drive the same per-layer arithmetic):
+ *  RESTART: every layer propagates the INPUT track to that layer's hit and updates the
+ *           output, so only the last layer determines the result (TBB:880-911).
+ *  CHAINED: the state is carried from layer to layer (a Kalman filter; the chained GPU
+ *           variants, cuda_v4.cu:840-846). */
+typedef enum p2r_mode { P2R_MODE_RESTART = 0, P2R_MODE_CHAINED = 1 } p2r_mode;
+
+/* Option bits for p2r_config.flags. */
+#define P2R_FLAG_FP32_DET 0x1u   /* 2x2 residual-covariance determinant in FP32 (default FP64, TBB:457) */
+#define P2R_FLAG_NO_STAGING 0x2u /* read hits with plain loads instead of cp.async staging */
+
+typedef struct p2r_config {
+  int32_t bsize;         /* Matriplex lanes per block (TBB:15-17); >= 1 */
+  int32_t nlayer;        /* hit blocks per track block (TBB:32-34); >= 1 */
+  int64_t nevts;         /* events (TBB:24-26) */
+  int64_t nb;            /* track blocks per event, ntrks/bsize (TBB:22) */
+  double bz;             /* field [T]; kfact = float(100/(-0.299792458*bz)) (TBB:654); 0 -> 3.8112 */
+  int32_t mode;          /* p2r_mode */
+  uint32_t flags;        /* P2R_FLAG_* */
+  int32_t block_threads; /* threads per CTA, multiple of 32 (0 = library default) */
+  int32_t stages;        /* hit-staging pipeline depth, 2 or 4 (0 = library default, 4) */
+} p2r_config;
+
+/* Returns P2R_ABI_VERSION. */
+int p2r_abi_version(void);
+
+/* Message of the calling thread's last error ("" if none). */
+const char* p2r_last_error_string(void);
+
+/* kfact for a field of bz tesla, rounded to float as TBB:654 rounds its constant. */
+float p2r_kfact(double bz);
+
+/* ---------------------------------------------------------------- per-layer (drop-in)
+ * Replaces one call of propagateToR(&in->cov, &in->par, &in->q, &hit->pos, &out->cov,
+ * &out->par) (TBB:656-812, called at TBB:894) for EVERY block b in [0, nevts*nb):
+ * in = trk_in[b], hit = hits[layer + b*nlayer], out = trk_out[b]. trk_out's q is copied
+ * from trk_in. trk_in may equal trk_out (the chained drivers' in-place call,
+ * cuda_v4.cu:843). dr (nullable, nlayer floats) adds dr[layer] cm to the target radius. */
+int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hits, int32_t layer,
+                       void* trk_out, const float* dr, void* stream);
+
+/* Replaces one call of KalmanUpdate(&trk->cov, &trk->par, &hit->cov, &hit->pos)
+ * (TBB:433-642, called at TBB:911) for every block b: trk[b] updated in place with
+ * hits[layer + b*nlayer]. chi2_accum (nullable, one float per track, track index
+ * b*bsize + lane) gets the update's chi2 added (the reference's commented-out
+ * Chi2Similarity, TBB:631). */
+int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_t layer, float* chi2_accum,
+                      void* stream);
+
+/* ---------------------------------------------------------------- fused driver
+ * The whole driver loop (TBB:873-926 for one iteration) in one launch: every track runs
+ * all nlayer (propagate, update) pairs with its state in registers, reading each hit once.
+ * trk_out may not alias trk_in. chi2_out (nullable) receives the summed chi2 per track.
+ * dr (nullable, nlayer floats) as in p2r_propagate_to_r. In RESTART mode only the last
+ * layer determines the result (TBB:894 overwrites the output each layer), and only that
+ * layer is computed. */
+int p2r_forward(const p2r_config* cfg, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
+                const float* dr, void* stream);
+
+/* Chained forward over blocks whose lanes carry their own layer counts: lane `it` of
+ * block b runs layers [0, nlay_lane[b*bsize + it]) (values 0..cfg->nlayer), then keeps
+ * its state. The reference has no uneven-layer form; at nlay_lane[] == nlayer this equals
+ * p2r_forward in CHAINED mode. */
+int p2r_forward_masked(const p2r_config* cfg, const void* trk_in, const void* hits, void* trk_out,
+                       const int32_t* nlay_lane, float* chi2_out, const float* dr, void* stream);
+
+/* Number of tracks with a non-finite x, y, z, 1/pT, phi or theta among nblocks blocks
+ * of trk (the reference's nnans, TBB:952-960), written to *count_out (device int64,
+ * accumulated with atomics: zero it first). */
+int p2r_count_nonfinite(const void* trk, int64_t nblocks, int32_t bsize, unsigned long long* count_out,
+                        void* stream);
+
+/* Host-buffer driver: p2r_forward over HOST arrays (host_trk_in, host_hits -> host_trk_out)
+ * through caller-provided device arrays of the full size. Events are split into nchunks
+ * contiguous chunks; each chunk's H2D copy, fused forward and D2H copy are queued on a
+ * library-owned pool of three streams so copies overlap kernels (the reference's
+ * multi-stream driver, cuda_v4.cu:912-1010). Ordered after prior work on `stream`, and
+ * `stream` waits for all of it. Host arrays should be pinned for the copies to overlap.
+ * The first call on a device creates the pool (streams and events, no device memory). */
+int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void* host_hits, void* host_trk_out,
+                     void* dev_trk_in, void* dev_hits, void* dev_trk_out, int32_t nchunks, void* stream);
+
+/* ---------------------------------------------------------------- measurement helper
+ * FP32 FMA throughput probe (the denominator of the FP32 compute roofline): blocks x
+ * threads threads each run 8 independent FMA chains for 4*iters rounds; FLOPs per launch
+ * = 64 * iters * blocks * threads. out: blocks*threads floats. threads: 32..256. */
+int p2r_fp32_fma_probe(int64_t iters, int32_t blocks, int32_t threads, float* out, void* stream);
+
+/* ---------------------------------------------------------------- host-side helpers */
+
+/* Parameters of the synthetic helix generator (p2r_gen_helix).
+ * Track population: true helices from the origin with pT = pt*(1 + pop_smear*N(0,1)),
+ * phi uniform in [-pi, pi], theta uniform in [theta_min, theta_max], charge +-1 with equal
+ * probability; the seed is the true state where the helix crosses
+ * r_seed*(1 + pop_smear*N(0,1)). The initial estimate handed to the filter is the seed
+ * displaced by est_smear standard deviations of the diagonal seed covariance
+ * (cov_pos for x, y, z; cov_ang for 1/pT, phi, theta). Hits: the helix crossing the
+ * cylinders r_first..r_last (equally spaced), smeared by hit_sigma per coordinate, with
+ * covariance hit_sigma^2 * I. */
+typedef struct p2r_gen_params {
+  uint64_t seed;
+  double bz;                   /* field [T] */
+  double r_seed;               /* nominal seed radius [cm] */
+  double r_first, r_last;      /* hit cylinders [cm] */
+  double pt;                   /* nominal pT [GeV] */
+  double pop_smear;            /* relative Gaussian spread of pT and seed radius over the population */
+  double theta_min, theta_max; /* polar-angle range [rad] */
+  double cov_pos, cov_ang;     /* seed covariance diagonal [cm^2] and [GeV^-2, rad^2] */
+  double est_smear;            /* displacement of the initial estimate, in seed-covariance sigmas */
+  double hit_sigma;            /* hit smear per coordinate [cm] */
+} p2r_gen_params;
+
+/* Defaults: 3.8 T, seeds near r = 15 cm, hits on r = 20..100 cm, pT near 4 GeV, 10 %
+ * population spread, theta 0.3..2.8, seed cov diag 1e-4 / 1e-3, estimates displaced by
+ * one sigma draw, 10 um hits. */
+void p2r_gen_params_default(p2r_gen_params* gp);
+
+/* Fills HOST arrays host_trk (nevts*nb MPTRK blocks) and host_hits (nevts*nb*nlayer MPHIT
+ * blocks), geometry in FP64 (see p2r_gen_params). ntrk_event (nullable, nevts entries):
+ * tracks per event; lanes past it are padding and carry their undisplaced true seed.
+ * Deterministic for a given seed and any nthreads (<= 0: all host threads). */
+int p2r_gen_helix(const p2r_gen_params* gp, int32_t bsize, int64_t nevts, int64_t nb, int32_t nlayer,
+                  const int32_t* ntrk_event, void* host_trk, void* host_hits, int32_t nthreads);
+
+/* The reference's input recipe (prepareTracks / prepareHits, TBB:243-293 with randn
+ * TBB:127-145) on HOST arrays, from a caller-supplied seed track (par[6], cov[21], q) and
+ * n_input_hits hits (pos[3], cov[6] each, in layer order). Draws from glibc rand() in the
+ * reference's order; call srand(1) first to reproduce a fresh run of the reference. */
+int p2r_gen_fixture(const float* seed_par6, const float* seed_cov21, int32_t seed_q, const float* hits_lx9,
+                    int32_t n_input_hits, int32_t bsize, int64_t nevts, int64_t nb, int32_t nlayer, double smear,
+                    void* host_trk, void* host_hits);
+
+/* The reference's end-of-run validation summary (TBB:935-1048) over HOST output tracks,
+ * against the last layer's unsmeared hit position host_hit_xyz[3]. */
+typedef struct p2r_summary_stats {
+  double avg_x, avg_y, avg_z, avg_r, avg_pt, avg_phi, avg_theta;
+  double avg_dx, avg_dy, avg_dz, avg_dr;
+  double std_x, std_y, std_z, std_r, std_dx, std_dy, std_dz, std_dr;
+  int64_t nnans, nfail;
+} p2r_summary_stats;
+
+int p2r_summary(const void* host_trk, int32_t bsize, int64_t nevts, int64_t nb, const float* host_hit_xyz,
+                p2r_summary_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* P2R_B200_H */

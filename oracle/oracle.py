@@ -1,0 +1,164 @@
+"""ctypes access to the oracle libraries.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline / reference arm, always as the checker or the timed CPU reference, never by
+the product package.
+
+  Oracle      the project's own CPU restatement (p2r_oracle.cpp), float and double
+  RefTBB      the reference's CPU path compiled unmodified (ref_harness.cpp -> _ref/)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "_build" / "libp2r_oracle.so"
+REF_DIR = HERE / "_ref"
+
+_vp = ctypes.c_void_p
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+class Oracle:
+    """Own restatement. run(..., prec='f32'|'f64') -> dict(out (float32 MPTRK), par, cov, chi2,
+    prior = covariance entering the last update)."""
+
+    def __init__(self, path: Path = ORACLE_LIB):
+        if not path.exists():
+            raise RuntimeError(f"{path} missing: build it with `make -C oracle oracle`")
+        self.l = ctypes.CDLL(str(path))
+        sig = [_vp, _vp, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _vp, _vp,
+               _vp, _vp, _vp, _vp, _vp]
+        for n in ("orc_run_f32", "orc_run_f64"):
+            getattr(self.l, n).argtypes = sig
+            getattr(self.l, n).restype = None
+        self.l.orc_step_f64.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp, _vp]
+        self.l.orc_step_f64.restype = ctypes.c_double
+        self.l.orc_kfact_f32.argtypes = [ctypes.c_double]
+        self.l.orc_kfact_f32.restype = ctypes.c_float
+
+    def run(self, trk: np.ndarray, hit: np.ndarray, bsize: int, nlayer: int, mode: int, bz: float,
+            prec: str = "f64", dr=None, nlay_lane=None) -> dict:
+        trk = np.ascontiguousarray(trk, np.float32)
+        hit = np.ascontiguousarray(hit, np.float32)
+        nblocks = trk.size // (28 * bsize)
+        ntr = nblocks * bsize
+        out = np.empty_like(trk)
+        par = np.empty((ntr, 6))
+        cov = np.empty((ntr, 21))
+        chi2 = np.empty(ntr)
+        prior = np.zeros((ntr, 21))
+        drv = None if dr is None else np.ascontiguousarray(dr, np.float64)
+        nl = None if nlay_lane is None else np.ascontiguousarray(nlay_lane, np.int32)
+        fn = self.l.orc_run_f32 if prec == "f32" else self.l.orc_run_f64
+        fn(trk.ctypes.data, hit.ctypes.data, nblocks, bsize, nlayer, mode, bz, _p(drv), _p(nl), out.ctypes.data,
+           par.ctypes.data, cov.ctypes.data, chi2.ctypes.data, prior.ctypes.data)
+        return {"out": out, "par": par, "cov": cov, "chi2": chi2, "prior": prior}
+
+    def step_f64(self, par, cov, q, hitpos, hitcov, dr, bz):
+        par = np.ascontiguousarray(par, np.float64)
+        cov = np.ascontiguousarray(cov, np.float64)
+        hp = np.ascontiguousarray(hitpos, np.float64)
+        hc = np.ascontiguousarray(hitcov, np.float64)
+        po = np.empty(6)
+        co = np.empty(21)
+        chi2 = self.l.orc_step_f64(par.ctypes.data, cov.ctypes.data, int(q), hp.ctypes.data, hc.ctypes.data,
+                                   float(dr), float(bz), po.ctypes.data, co.ctypes.data)
+        return po, co, chi2
+
+
+def host_isa() -> str:
+    """'v4' when the host CPU has AVX-512 (F, BW, VL, DQ, CD), else 'v3'."""
+    try:
+        flags = set()
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+        need = {"avx512f", "avx512bw", "avx512vl", "avx512dq", "avx512cd"}
+        return "v4" if need <= flags else "v3"
+    except OSError:
+        return "v3"
+
+
+def ref_available(bsize: int = 32, kind: str | None = None) -> bool:
+    return (REF_DIR / f"libp2r_tbbref_b{bsize}_{kind or host_isa()}.so").exists()
+
+
+class RefTBB:
+    """The reference's own CPU functions (TBB:433-812) and driver loop, one build per bsize.
+
+    kind: 'v3' / 'v4' = unmodified source (kfact fixed at 3.8112 T), 'kf' = run-time kfact.
+    """
+
+    def __init__(self, bsize: int = 32, kind: str | None = None):
+        kind = kind or host_isa()
+        path = REF_DIR / f"libp2r_tbbref_b{bsize}_{kind}.so"
+        if not path.exists():
+            raise RuntimeError(f"{path} missing: build it with `make -C oracle ref` where the reference exists")
+        self.bsize = bsize
+        self.kind = kind
+        self.l = ctypes.CDLL(str(path))
+        L = self.l
+        L.ref_run.argtypes = [_vp, _vp, _vp, ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_int]
+        L.ref_run_masked.argtypes = [_vp, _vp, _vp, ctypes.c_long, ctypes.c_int, _vp]
+        L.ref_set_bz.argtypes = [ctypes.c_double]
+        L.ref_get_kfact.restype = ctypes.c_float
+        L.ref_propagate_block.argtypes = [_vp, _vp, _vp]
+        L.ref_update_block.argtypes = [_vp, _vp]
+        L.ref_prepare_fixture.argtypes = [_vp, _vp]
+        L.ref_fixture_raw.argtypes = [_vp, _vp, _vp, _vp]
+        for n in ("ref_fixture_nevts", "ref_fixture_ntrks", "ref_fixture_nb"):
+            getattr(L, n).restype = ctypes.c_long
+
+    def set_bz(self, bz: float) -> None:
+        if self.l.ref_set_bz(bz) != 0:
+            raise ValueError(f"this reference build has kfact fixed at 3.8112 T; use kind='kf' for bz={bz}")
+
+    def run(self, trk, hit, nevts, nb, nlayer, chained, niter=1, nthreads=1):
+        trk = np.ascontiguousarray(trk, np.float32)
+        hit = np.ascontiguousarray(hit, np.float32)
+        out = np.empty_like(trk)
+        self.l.ref_run(trk.ctypes.data, hit.ctypes.data, out.ctypes.data, nevts, nb, nlayer, niter, nthreads,
+                       1 if chained else 0)
+        return out
+
+    def run_into(self, trk, hit, out, nevts, nb, nlayer, chained, niter=1, nthreads=1):
+        self.l.ref_run(trk.ctypes.data, hit.ctypes.data, out.ctypes.data, nevts, nb, nlayer, niter, nthreads,
+                       1 if chained else 0)
+
+    def run_masked(self, trk, hit, nlayer_max, nlay_lane):
+        trk = np.ascontiguousarray(trk, np.float32)
+        hit = np.ascontiguousarray(hit, np.float32)
+        nl = np.ascontiguousarray(nlay_lane, np.int32)
+        out = np.empty_like(trk)
+        nblocks = trk.size // (28 * self.bsize)
+        self.l.ref_run_masked(trk.ctypes.data, hit.ctypes.data, out.ctypes.data, nblocks, nlayer_max, nl.ctypes.data)
+        return out
+
+    def fixture_sizes(self):
+        return int(self.l.ref_fixture_nevts()), int(self.l.ref_fixture_nb()), int(self.l.ref_fixture_nlayer())
+
+    def prepare_fixture(self):
+        nev, nb, nl = self.fixture_sizes()
+        trk = np.empty(nev * nb * 28 * self.bsize, np.float32)
+        hit = np.empty(nev * nb * nl * 9 * self.bsize, np.float32)
+        self.l.ref_prepare_fixture(trk.ctypes.data, hit.ctypes.data)
+        return trk, hit
+
+    def fixture_raw(self):
+        par = np.empty(6, np.float32)
+        cov = np.empty(21, np.float32)
+        q = np.zeros(1, np.int32)
+        hits = np.empty((22, 9), np.float32)
+        self.l.ref_fixture_raw(par.ctypes.data, cov.ctypes.data, q.ctypes.data, hits.ctypes.data)
+        return par, cov, int(q[0]), hits

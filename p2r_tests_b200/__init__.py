@@ -1,0 +1,17 @@
+"""p2r-b200: B200-native (sm_100a) helix propagation + Kalman update over Matriplex arrays.
+
+The package `p2r-tests_b200` is spelled `p2r_tests_b200` because Python module names
+cannot contain '-'. The compute path is libp2r_b200.so (hand-written CUDA behind the C ABI
+in include/p2r.h); this package is the Python host side over that ABI.
+"""
+from ._lib import (FLAG_FP32_DET, FLAG_NO_STAGING, MODE_CHAINED, MODE_RESTART, P2RError, LIB_PATH, lib)
+from .api import (Config, KalmanUpdate, REF_BZ, count_nonfinite, forward, forward_host, fp32_fma_probe, gen_params,
+                  generate_fixture,
+                  generate_helix, kfact, propagateToR, run_layers, summary, tracks_cov, tracks_par, tracks_q)
+
+__all__ = [
+    "Config", "KalmanUpdate", "propagateToR", "run_layers", "forward", "forward_host", "fp32_fma_probe",
+    "count_nonfinite", "kfact",
+    "gen_params", "generate_helix", "generate_fixture", "summary", "tracks_par", "tracks_cov", "tracks_q",
+    "MODE_CHAINED", "MODE_RESTART", "FLAG_FP32_DET", "FLAG_NO_STAGING", "P2RError", "REF_BZ", "LIB_PATH", "lib",
+]

@@ -1,0 +1,98 @@
+"""Builds the in-tree CUDA library libp2r_b200.so for sm_100a (and the CPU oracle).
+
+nvcc cross-compiles for sm_100a without a GPU, so this runs on any host with the CUDA
+toolkit. Objects go to p2r_tests_b200/_build/, the library to p2r_tests_b200/.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libp2r_b200.so"
+ROOT = PKG.parent
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+              "--expt-relaxed-constexpr", "-I" + str(ROOT / "include")]
+CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-I" + str(ROOT / "include")]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libp2r_b200.so")
+
+
+def cuda_home() -> Path:
+    return Path(nvcc()).resolve().parent.parent
+
+
+def sources() -> list[Path]:
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
+
+
+def headers() -> list[Path]:
+    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "p2r.h"])
+
+
+def _compile(src: Path, verbose_ptxas: bool) -> tuple[Path, str]:
+    obj = BUILD / (src.name + ".o")
+    if src.suffix == ".cu":
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+        if verbose_ptxas:
+            cmd += ["-Xptxas", "-v"]
+    else:
+        cmd = [os.environ.get("CXX", "g++"), *CXX_FLAGS, "-I" + str(cuda_home() / "include"),
+               "-c", str(src), "-o", str(obj)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+    return obj, res.stdout + res.stderr
+
+
+def build_library(force: bool = False, verbose_ptxas: bool = False, quiet: bool = True) -> Path:
+    """Compiles every csrc/ source for sm_100a and links libp2r_b200.so (incremental)."""
+    BUILD.mkdir(exist_ok=True)
+    srcs = sources()
+    newest = max(p.stat().st_mtime for p in srcs + headers() + [Path(__file__)])
+    if LIB.exists() and not force and not verbose_ptxas and LIB.stat().st_mtime >= newest:
+        return LIB
+    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda s: _compile(s, verbose_ptxas), srcs))
+    for _, log in results:
+        if log.strip() and not quiet:
+            print(log, file=sys.stderr)
+    objs = [str(o) for o, _ in results]
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"link failed: {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def build_oracle() -> None:
+    """Builds oracle/_build (always) and oracle/_ref (only where the reference checkout exists)."""
+    make = shutil.which("make")
+    if make is None:
+        raise RuntimeError("make not found")
+    subprocess.run([make, "-s", "-C", str(ROOT / "oracle"), "oracle"], check=True)
+    refdir = Path(os.environ.get("P2R_REFDIR", "/root/reference"))
+    if (refdir / "src" / "propagate-tor-test_tbb.cpp").exists():
+        subprocess.run([make, "-s", "-C", str(ROOT / "oracle"), "ref", f"REFDIR={refdir}"], check=True)
+
+
+if __name__ == "__main__":
+    build_library(force="--force" in sys.argv, verbose_ptxas="-v" in sys.argv, quiet=False)
+    if "--oracle" in sys.argv:
+        build_oracle()
+    print(LIB)

@@ -1,0 +1,206 @@
+// C-ABI entry points of the forward path: the fused driver (p2r_forward, p2r_forward_masked)
+// and the per-layer kernels that mirror the reference's call shape:
+//  propagate_kernel  one propagateToR per track for one layer (TBB:894)
+//  update_kernel     one KalmanUpdate per track for one layer (TBB:911)
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "p2r_fwd.cuh"
+#include "p2r_internal.h"
+
+namespace p2r {
+
+// ---------------------------------------------------------------- per-layer kernels
+__global__ void __launch_bounds__(128) propagate_kernel(const float* trk_in, const float* hits, float* trk_out,
+                                                        const float* dr, long long nblocks, int bs, int nlayer,
+                                                        int layer, float kfact) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long b = g / bs;
+  const int it = (int)(g - b * bs);
+  if (b >= nblocks) return;
+  // trk_in may alias trk_out: plain loads, all inputs read before any store.
+  const float* blk = trk_in + b * (long long)(kTrkWords * bs);
+  float par[6], cov[21];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) par[i] = blk[i * bs + it];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) cov[i] = blk[(6 + i) * bs + it];
+  const float qf = blk[27 * bs + it];
+  const float k = (float)__float_as_int(qf) * kfact;
+  const float* h = hits + (b * nlayer + layer) * (long long)(kHitWords * bs);
+  const float rh = hipo(h[it], h[bs + it]);
+  const float rt = dr ? rh + dr[layer] : rh;
+  float op[6], oc[21];
+  propagate_to_r(par, cov, k, 1.f / k, rt, op, oc);
+  float* ob = trk_out + b * (long long)(kTrkWords * bs);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) ob[i * bs + it] = op[i];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) ob[(6 + i) * bs + it] = oc[i];
+  ob[27 * bs + it] = qf;
+}
+
+template <bool FP64DET>
+__global__ void __launch_bounds__(128) update_kernel(float* trk, const float* hits, float* chi2_accum, long long nblocks,
+                                                     int bs, int nlayer, int layer) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long b = g / bs;
+  const int it = (int)(g - b * bs);
+  if (b >= nblocks) return;
+  float* blk = trk + b * (long long)(kTrkWords * bs);
+  float par[6], cov[21];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) par[i] = blk[i * bs + it];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) cov[i] = blk[(6 + i) * bs + it];
+  const float* h = hits + (b * nlayer + layer) * (long long)(kHitWords * bs);
+  float hp[3], hc[6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) hp[i] = h[i * bs + it];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) hc[i] = h[(3 + i) * bs + it];
+  const float rh = hipo(hp[0], hp[1]);
+  float chi2;
+  if (chi2_accum)
+    chi2 = kalman_update<FP64DET, true>(par, cov, hp, hc, rh);
+  else
+    chi2 = kalman_update<FP64DET, false>(par, cov, hp, hc, rh);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) blk[i * bs + it] = par[i];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) blk[(6 + i) * bs + it] = cov[i];
+  if (chi2_accum) chi2_accum[b * bs + it] += chi2;
+}
+
+__global__ void count_nonfinite_kernel(const float* trk, long long nblocks, int bs, unsigned long long* count) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long b = g / bs;
+  const int it = (int)(g - b * bs);
+  bool bad = false;
+  if (b < nblocks) {
+    const float* blk = trk + b * (long long)(kTrkWords * bs);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) bad |= !isfinite(blk[i * bs + it]);
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(count, (unsigned long long)__popc(m));
+}
+
+}  // namespace p2r
+
+
+using namespace p2r;
+
+static int check_ptr16(const void* ptr) { return ((uintptr_t)ptr & 15u) == 0; }
+
+static int forward_impl(const p2r_config* cfg, const void* trk_in, const void* hits, void* trk_out,
+                        const int32_t* nlay, float* chi2_out, const float* dr, void* stream, const char* who) {
+  int rc = p2r_check_config(cfg, who);
+  if (rc) return rc;
+  const long long nblocks = (long long)cfg->nevts * cfg->nb;
+  if (nblocks == 0) return p2r_clear_error();  // an empty batch is valid (pointers unused)
+  if (!trk_in || !hits || !trk_out) return p2r_set_errorf(P2R_ERR_INVALID, "%s: null array pointer", who);
+  if (trk_in == trk_out) return p2r_set_errorf(P2R_ERR_INVALID, "%s: trk_out may not alias trk_in", who);
+  if (cfg->mode != P2R_MODE_RESTART && cfg->mode != P2R_MODE_CHAINED)
+    return p2r_set_errorf(P2R_ERR_INVALID, "%s: unknown mode %d", who, cfg->mode);
+  if (nlay && cfg->mode != P2R_MODE_CHAINED)
+    return p2r_set_errorf(P2R_ERR_INVALID, "%s: per-lane layer counts need CHAINED mode", who);
+  FwdParams p;
+  p.trk_in = (const float*)trk_in;
+  p.hits = (const float*)hits;
+  p.trk_out = (float*)trk_out;
+  p.chi2 = chi2_out;
+  p.dr = dr;
+  p.nlay = nlay;
+  p.nblocks = nblocks;
+  p.bsize = cfg->bsize;
+  p.nlayer = cfg->nlayer;
+  p.kfact = p2r_kfact_of(cfg->bz);
+  const int threads = cfg->block_threads > 0 ? cfg->block_threads : 128;
+  if (threads % 32 || threads > 128)
+    return p2r_set_errorf(P2R_ERR_INVALID, "%s: block_threads must be a multiple of 32 up to 128", who);
+  const int stages = cfg->stages > 0 ? cfg->stages : 4;
+  if (stages != 2 && stages != 4) return p2r_set_errorf(P2R_ERR_INVALID, "%s: stages must be 2 or 4", who);
+  const bool staged = !(cfg->flags & P2R_FLAG_NO_STAGING) && cfg->bsize % 32 == 0 && check_ptr16(hits);
+  const bool fp64det = !(cfg->flags & P2R_FLAG_FP32_DET);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if (cfg->mode == P2R_MODE_RESTART)
+    e = launch_restart(p, fp64det, threads, stages, st);
+  else if (nlay)
+    e = launch_masked(p, staged, fp64det, threads, stages, st);
+  else
+    e = launch_chained(p, staged, fp64det, threads, stages, st);
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: launch failed: %s", who, cudaGetErrorString(e));
+  return p2r_clear_error();
+}
+
+extern "C" {
+
+int p2r_forward(const p2r_config* cfg, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
+                const float* dr, void* stream) {
+  return forward_impl(cfg, trk_in, hits, trk_out, nullptr, chi2_out, dr, stream, "p2r_forward");
+}
+
+int p2r_forward_masked(const p2r_config* cfg, const void* trk_in, const void* hits, void* trk_out,
+                       const int32_t* nlay_lane, float* chi2_out, const float* dr, void* stream) {
+  if (!nlay_lane) return p2r_set_error(P2R_ERR_INVALID, "p2r_forward_masked: nlay_lane is null");
+  return forward_impl(cfg, trk_in, hits, trk_out, nlay_lane, chi2_out, dr, stream, "p2r_forward_masked");
+}
+
+int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hits, int32_t layer, void* trk_out,
+                       const float* dr, void* stream) {
+  int rc = p2r_check_config(cfg, "p2r_propagate_to_r");
+  if (rc) return rc;
+  if (!trk_in || !hits || !trk_out) return p2r_set_error(P2R_ERR_INVALID, "p2r_propagate_to_r: null array pointer");
+  if (layer < 0 || layer >= cfg->nlayer)
+    return p2r_set_errorf(P2R_ERR_INVALID, "p2r_propagate_to_r: layer %d outside [0, %d)", layer, cfg->nlayer);
+  const long long nblocks = (long long)cfg->nevts * cfg->nb;
+  if (nblocks == 0) return p2r_clear_error();
+  const long long ntr = nblocks * cfg->bsize;
+  const int threads = 128;
+  propagate_kernel<<<(unsigned)((ntr + threads - 1) / threads), threads, 0, (cudaStream_t)stream>>>(
+      (const float*)trk_in, (const float*)hits, (float*)trk_out, dr, nblocks, cfg->bsize, cfg->nlayer, layer,
+      p2r_kfact_of(cfg->bz));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_propagate_to_r: %s", cudaGetErrorString(e));
+  return p2r_clear_error();
+}
+
+int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_t layer, float* chi2_accum,
+                      void* stream) {
+  int rc = p2r_check_config(cfg, "p2r_kalman_update");
+  if (rc) return rc;
+  if (!trk || !hits) return p2r_set_error(P2R_ERR_INVALID, "p2r_kalman_update: null array pointer");
+  if (layer < 0 || layer >= cfg->nlayer)
+    return p2r_set_errorf(P2R_ERR_INVALID, "p2r_kalman_update: layer %d outside [0, %d)", layer, cfg->nlayer);
+  const long long nblocks = (long long)cfg->nevts * cfg->nb;
+  if (nblocks == 0) return p2r_clear_error();
+  const long long ntr = nblocks * cfg->bsize;
+  const int threads = 128;
+  const unsigned grid = (unsigned)((ntr + threads - 1) / threads);
+  if (cfg->flags & P2R_FLAG_FP32_DET)
+    update_kernel<false><<<grid, threads, 0, (cudaStream_t)stream>>>((float*)trk, (const float*)hits, chi2_accum,
+                                                                      nblocks, cfg->bsize, cfg->nlayer, layer);
+  else
+    update_kernel<true><<<grid, threads, 0, (cudaStream_t)stream>>>((float*)trk, (const float*)hits, chi2_accum,
+                                                                     nblocks, cfg->bsize, cfg->nlayer, layer);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_kalman_update: %s", cudaGetErrorString(e));
+  return p2r_clear_error();
+}
+
+int p2r_count_nonfinite(const void* trk, int64_t nblocks, int32_t bsize, unsigned long long* count_out, void* stream) {
+  if (!trk || !count_out) return p2r_set_error(P2R_ERR_INVALID, "p2r_count_nonfinite: null pointer");
+  if (nblocks < 0 || bsize < 1) return p2r_set_error(P2R_ERR_INVALID, "p2r_count_nonfinite: bad sizes");
+  if (nblocks == 0) return p2r_clear_error();
+  const long long ntr = nblocks * (long long)bsize;
+  const int threads = 256;
+  count_nonfinite_kernel<<<(unsigned)((ntr + threads - 1) / threads), threads, 0, (cudaStream_t)stream>>>(
+      (const float*)trk, nblocks, bsize, count_out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_count_nonfinite: %s", cudaGetErrorString(e));
+  return p2r_clear_error();
+}
+
+}  // extern "C"

@@ -1,0 +1,342 @@
+"""GPU parity tests: the CUDA path (through the C ABI) against the reference's own CPU code.
+
+Comparisons use the reference's compiled functions (oracle/_ref, built from
+src/propagate-tor-test_tbb.cpp) where present, and the committed golden vectors it
+produced otherwise; the FP64 restatement (oracle/) measures accuracy. Tolerances and
+metrics: tests/parity.py.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from tests import parity
+
+pytestmark = pytest.mark.gpu
+
+MODES = {"restart": 0, "chained": 1}
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def gpu_forward(p2r, torch, cfg, trk, hit, chi2=False, dr=None, nlay_lane=None):
+    dt, dh = dev(torch, trk), dev(torch, hit)
+    out = torch.empty_like(dt)
+    c2 = torch.zeros(cfg.ntracks, dtype=torch.float32, device="cuda") if chi2 else None
+    ddr = None if dr is None else dev(torch, np.asarray(dr, np.float32))
+    dnl = None if nlay_lane is None else dev(torch, np.asarray(nlay_lane, np.int32))
+    p2r.forward(cfg, dt, dh, out, chi2=c2, dr=ddr, nlay_lane=dnl)
+    torch.cuda.synchronize()
+    return (host(out), host(c2)) if chi2 else host(out)
+
+
+def ref_or_none(bs, kind):
+    from oracle.oracle import RefTBB, ref_available
+    return RefTBB(bs, kind) if ref_available(bs, kind) else None
+
+
+def fixture(p2r, golden_dir, bs):
+    g = dict(np.load(golden_dir / f"ref_fixture_b{bs}.npz"))
+    fx = dict(np.load(golden_dir / "fixture.npz"))
+    cfg = p2r.Config(bsize=bs, nlayer=int(g["nlayer"]), nevts=int(g["nevts"]), nb=int(g["nb"]), bz=p2r.REF_BZ)
+    ctypes.CDLL("libc.so.6").srand(1)
+    trk, hit = p2r.generate_fixture(fx["par"], fx["cov"], int(fx["q"]), fx["hits"], cfg, smear=1e-5)
+    return cfg, trk, hit, g
+
+
+def helix(p2r, nevts, nb, nlayer=20, bs=32, bz=3.8, seed=20240001):
+    cfg = p2r.Config(bsize=bs, nlayer=nlayer, nevts=nevts, nb=nb, bz=bz)
+    trk, hit = p2r.generate_helix(cfg, p2r.gen_params(bz=bz, seed=seed))
+    return cfg, trk, hit
+
+
+def slice_layer(hit, nblocks, nlayer, layer, bs):
+    return np.ascontiguousarray(hit.reshape(nblocks, nlayer, 9, bs)[:, layer:layer + 1])
+
+
+# ---------------------------------------------------------------------------- fixture
+@pytest.mark.parametrize("bs", [32, 64, 128])
+def test_fixture_restart_matches_reference(p2r, oracle, torch, golden_dir, bs):
+    cfg, trk, hit, g = fixture(p2r, golden_dir, bs)
+    cfg.mode = p2r.MODE_RESTART
+    out = gpu_forward(p2r, torch, cfg, trk, hit)
+    f64 = oracle.run(trk, hit, bs, cfg.nlayer, 0, cfg.bz, "f64")
+    parity.assert_elementwise(out, g["out_restart"], f64["prior"], bs, f"GPU restart b{bs} vs reference")
+
+
+@pytest.mark.parametrize("bs", [32, 64, 128])
+def test_fixture_chained_matches_reference(p2r, oracle, torch, golden_dir, bs):
+    cfg, trk, hit, g = fixture(p2r, golden_dir, bs)
+    out = gpu_forward(p2r, torch, cfg, trk, hit)
+    f64 = oracle.run(trk, hit, bs, cfg.nlayer, 1, cfg.bz, "f64")
+    tp, _, tq = parity.unpack(out, bs)
+    _, _, rq = parity.unpack(g["out_chained"], bs)
+    assert np.array_equal(tq, rq)
+    assert np.isfinite(tp).all()
+    parity.assert_accuracy_parity(out, g["out_chained"], f64["par"], f64["cov"], f64["prior"], bs,
+                                  f"GPU chained b{bs} (fixture)", factor=4.0)
+
+
+# ---------------------------------------------------------------------------- helix workload
+@pytest.mark.parametrize("mode", list(MODES))
+def test_helix_golden(p2r, oracle, torch, golden_dir, mode):
+    g = dict(np.load(golden_dir / "ref_helix.npz"))
+    bs, nl, bz = int(g["bsize"]), int(g["nlayer"]), float(g["bz"])
+    cfg = p2r.Config(bsize=bs, nlayer=nl, nevts=int(g["nevts"]), nb=int(g["nb"]), bz=bz, mode=MODES[mode])
+    out = gpu_forward(p2r, torch, cfg, g["trk"], g["hit"])
+    f64 = oracle.run(g["trk"], g["hit"], bs, nl, MODES[mode], bz, "f64")
+    if mode == "restart":
+        parity.assert_elementwise(out, g["out_restart"], f64["prior"], bs, "GPU restart (helix golden)")
+    else:
+        parity.assert_accuracy_parity(out, g["out_chained"], f64["par"], f64["cov"], f64["prior"], bs,
+                                      "GPU chained (helix golden)")
+
+
+@pytest.mark.parametrize("bs", [32, 64, 128])
+@pytest.mark.parametrize("mode", list(MODES))
+def test_helix_vs_live_reference(p2r, oracle, torch, bs, mode):
+    ref = ref_or_none(bs, "kf")
+    if ref is None:
+        pytest.skip("reference build not present")
+    nb = 9600 // bs // 10  # 960 tracks per event
+    cfg, trk, hit = helix(p2r, 4, nb, bs=bs)
+    cfg.mode = MODES[mode]
+    ref.set_bz(cfg.bz)
+    rout = ref.run(trk, hit, cfg.nevts, cfg.nb, cfg.nlayer, chained=bool(MODES[mode]))
+    out = gpu_forward(p2r, torch, cfg, trk, hit)
+    f64 = oracle.run(trk, hit, bs, cfg.nlayer, MODES[mode], cfg.bz, "f64")
+    if mode == "restart":
+        parity.assert_elementwise(out, rout, f64["prior"], bs, f"GPU restart b{bs} vs live reference")
+    else:
+        tp, tc, _ = parity.unpack(out, bs)
+        rp, rc, _ = parity.unpack(rout, bs)
+        ep = parity.rel_par(tp, rp)
+        ec = parity.rel_cov(tc, rc, f64["prior"])
+        assert np.quantile(ep, 0.99) <= parity.PAR_RTOL
+        assert np.quantile(ec, 0.99) <= parity.CHAIN_COV_P99
+        parity.assert_accuracy_parity(out, rout, f64["par"], f64["cov"], f64["prior"], bs,
+                                      f"GPU chained b{bs} vs live reference")
+
+
+def test_chained_step_parity_along_the_chain(p2r, oracle, torch):
+    """Every step of a chained run: reference state after layer l-1 in, one GPU propagate +
+    update with layer l, compared element-wise with the reference's state after layer l."""
+    ref = ref_or_none(32, "kf")
+    if ref is None:
+        pytest.skip("reference build not present")
+    cfg, trk, hit = helix(p2r, 2, 8)
+    ref.set_bz(cfg.bz)
+    nbk = cfg.nblocks
+    state = np.ascontiguousarray(trk.reshape(-1))
+    for l in range(cfg.nlayer):
+        h1 = slice_layer(hit, nbk, cfg.nlayer, l, 32)
+        want = ref.run(state, h1, cfg.nevts, cfg.nb, 1, chained=True)
+        c1 = p2r.Config(bsize=32, nlayer=1, nevts=cfg.nevts, nb=cfg.nb, bz=cfg.bz)
+        got = gpu_forward(p2r, torch, c1, state, h1)
+        f64 = oracle.run(state, h1, 32, 1, 1, cfg.bz, "f64")
+        parity.assert_elementwise(got, want, f64["prior"], 32, f"step {l}")
+        state = want
+
+
+@pytest.mark.parametrize("mode", list(MODES))
+def test_per_layer_calls_match_reference_steps(p2r, oracle, torch, mode):
+    """p2r_propagate_to_r / p2r_kalman_update: the reference's call shape, layer by layer."""
+    ref = ref_or_none(32, "kf")
+    if ref is None:
+        pytest.skip("reference build not present")
+    cfg, trk, hit = helix(p2r, 2, 8)
+    cfg.mode = MODES[mode]
+    ref.set_bz(cfg.bz)
+    nbk = cfg.nblocks
+    dt, dh = dev(torch, trk), dev(torch, hit)
+    out = torch.empty_like(dt)
+    out.copy_(dt)
+    state = np.ascontiguousarray(trk.reshape(-1))
+    for l in range(cfg.nlayer):
+        src = dt if mode == "restart" else out
+        p2r.propagateToR(cfg, src, dh, l, out)
+        p2r.KalmanUpdate(cfg, out, dh, l)
+        h1 = slice_layer(hit, nbk, cfg.nlayer, l, 32)
+        inp = trk.reshape(-1) if mode == "restart" else state
+        want = ref.run(inp, h1, cfg.nevts, cfg.nb, 1, chained=True)
+        f64 = oracle.run(inp, h1, 32, 1, 1, cfg.bz, "f64")
+        got = host(out)
+        parity.assert_elementwise(got, want, f64["prior"], 32, f"layer {l}")
+        out.copy_(dev(torch, want))  # continue from the reference state (step parity)
+        state = want
+
+
+def test_propagate_alone_matches_reference_block(p2r, torch):
+    """propagateToR alone (no update) against the reference's function on every block."""
+    ref = ref_or_none(32, "kf")
+    if ref is None:
+        pytest.skip("reference build not present")
+    cfg, trk, hit = helix(p2r, 1, 16)
+    ref.set_bz(cfg.bz)
+    dt, dh = dev(torch, trk), dev(torch, hit)
+    out = torch.empty_like(dt)
+    for l in (0, 7, 19):
+        p2r.propagateToR(cfg, dt, dh, l, out)
+        got = host(out).reshape(cfg.nblocks, 28, 32)
+        want = np.empty_like(got)
+        for b in range(cfg.nblocks):
+            tb = np.ascontiguousarray(trk[b])
+            hb = np.ascontiguousarray(hit[b * cfg.nlayer + l])
+            ob = np.empty_like(tb)
+            ref.l.ref_propagate_block(tb.ctypes.data, hb.ctypes.data, ob.ctypes.data)
+            want[b] = ob
+        _, wc, _ = parity.unpack(want, 32)
+        # no update: the output covariance itself is the conditioning scale
+        parity.assert_elementwise(got, want, wc, 32, f"propagate layer {l}")
+
+
+# ---------------------------------------------------------------------------- internal consistency
+def test_fused_chain_equals_per_layer_chain(p2r, torch):
+    cfg, trk, hit = helix(p2r, 3, 10)
+    fused = gpu_forward(p2r, torch, cfg, trk, hit)
+    dt, dh = dev(torch, trk), dev(torch, hit)
+    out = torch.empty_like(dt)
+    p2r.run_layers(cfg, dt, dh, out)
+    torch.cuda.synchronize()
+    a, b = fused.view(np.int32).astype(np.int64), host(out).view(np.int32).astype(np.int64)
+    ulps = np.abs(a - b)
+    assert np.quantile(ulps, 0.99) <= 64, np.quantile(ulps, [0.5, 0.99, 1.0])
+
+
+@pytest.mark.parametrize("bs", [32, 64, 128])
+def test_staged_equals_plain_loads(p2r, torch, bs):
+    cfg, trk, hit = helix(p2r, 2, 12 * 32 // bs, bs=bs)
+    a = gpu_forward(p2r, torch, cfg, trk, hit)
+    cfg.flags = p2r.FLAG_NO_STAGING
+    b = gpu_forward(p2r, torch, cfg, trk, hit)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("threads,stages", [(32, 2), (64, 4), (96, 4), (128, 2)])
+def test_launch_shapes_identical(p2r, torch, threads, stages):
+    cfg, trk, hit = helix(p2r, 2, 7)
+    base = gpu_forward(p2r, torch, cfg, trk, hit)
+    cfg.block_threads, cfg.stages = threads, stages
+    out = gpu_forward(p2r, torch, cfg, trk, hit)
+    assert np.array_equal(base.view(np.uint32), out.view(np.uint32))
+
+
+@pytest.mark.parametrize("bs_other", [1, 16, 64, 96])
+def test_layout_independence(p2r, torch, bs_other):
+    """Each track's result is independent of the Matriplex width it is stored in (indexing)."""
+    cfg32, trk, hit = helix(p2r, 1, 6, bs=32)
+    out32 = gpu_forward(p2r, torch, cfg32, trk, hit)
+    ntr = cfg32.ntracks
+    assert ntr % bs_other == 0
+    nb = ntr // bs_other
+
+    def relayout(a, words, nl, bs_from, bs_to):
+        x = a.reshape(-1, nl, words, bs_from).transpose(0, 3, 1, 2).reshape(-1, nl, words)  # (ntr, nl, words)
+        return np.ascontiguousarray(x.reshape(-1, bs_to, nl, words).transpose(0, 2, 3, 1))
+
+    trk_o = relayout(trk, 28, 1, 32, bs_other)
+    hit_o = relayout(hit, 9, cfg32.nlayer, 32, bs_other)
+    cfgo = p2r.Config(bsize=bs_other, nlayer=cfg32.nlayer, nevts=1, nb=nb, bz=cfg32.bz)
+    outo = gpu_forward(p2r, torch, cfgo, trk_o, hit_o)
+    back = relayout(outo, 28, 1, bs_other, 32)
+    assert np.array_equal(back.reshape(-1).view(np.uint32), out32.reshape(-1).view(np.uint32))
+
+
+def test_deterministic_and_q_copied(p2r, torch):
+    cfg, trk, hit = helix(p2r, 2, 50)
+    a = gpu_forward(p2r, torch, cfg, trk, hit)
+    b = gpu_forward(p2r, torch, cfg, trk, hit)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(parity.unpack(a, 32)[2], parity.unpack(trk, 32)[2])
+
+
+def test_empty_and_single_block(p2r, torch):
+    cfg = p2r.Config(bsize=32, nlayer=20, nevts=0, nb=4, bz=3.8)
+    e = torch.empty(0, device="cuda")
+    p2r.forward(cfg, e, e, torch.empty(0, device="cuda"))
+    cfg, trk, hit = helix(p2r, 1, 1)
+    out = gpu_forward(p2r, torch, cfg, trk, hit)
+    assert np.isfinite(parity.unpack(out, 32)[0]).all()
+
+
+def test_chi2_and_radius_offsets_match_oracle(p2r, oracle, torch):
+    cfg, trk, hit = helix(p2r, 2, 8)
+    rng = np.random.default_rng(7)
+    dr = rng.uniform(-0.01, 0.01, cfg.nlayer)  # +-100 um
+    for mode in (0, 1):
+        cfg.mode = mode
+        out, chi2 = gpu_forward(p2r, torch, cfg, trk, hit, chi2=True, dr=dr.astype(np.float32))
+        f64 = oracle.run(trk, hit, 32, cfg.nlayer, mode, cfg.bz, "f64", dr=dr.astype(np.float32).astype(np.float64))
+        rel = np.abs(chi2 - f64["chi2"]) / np.maximum(np.abs(f64["chi2"]), 1.0)
+        assert np.quantile(rel, 0.99) < 1e-3, np.quantile(rel, [0.5, 0.99, 1])
+        tp = parity.unpack(out, 32)[0]
+        assert np.quantile(parity.rel_par(tp, f64["par"]), 0.99) < parity.PAR_RTOL
+
+
+def test_masked_lanes_match_reference(p2r, oracle, torch):
+    ref = ref_or_none(32, "kf")
+    if ref is None:
+        pytest.skip("reference build not present")
+    cfg, trk, hit = helix(p2r, 2, 6, nlayer=25)
+    ref.set_bz(cfg.bz)
+    rng = np.random.default_rng(11)
+    nl = rng.integers(10, 26, cfg.ntracks).astype(np.int32)
+    nl[:32] = 25
+    nl[32:64] = 0  # a block whose lanes all stop at once
+    out = gpu_forward(p2r, torch, cfg, trk, hit, nlay_lane=nl)
+    want = ref.run_masked(trk, hit, cfg.nlayer, nl)
+    f64 = oracle.run(trk, hit, 32, cfg.nlayer, 1, cfg.bz, "f64", nlay_lane=nl)
+    parity.assert_accuracy_parity(out, want, f64["par"], f64["cov"], f64["prior"], 32, "masked lanes")
+    # lanes with 0 layers come back unchanged
+    assert np.array_equal(out.reshape(-1, 28, 32)[1].view(np.uint32), trk.reshape(-1, 28, 32)[1].view(np.uint32))
+
+
+def test_fp32_determinant_option(p2r, oracle, torch):
+    cfg, trk, hit = helix(p2r, 2, 20)
+    f64 = oracle.run(trk, hit, 32, cfg.nlayer, 1, cfg.bz, "f64")
+    d64 = gpu_forward(p2r, torch, cfg, trk, hit)
+    cfg.flags = p2r.FLAG_FP32_DET
+    d32 = gpu_forward(p2r, torch, cfg, trk, hit)
+    parity.assert_accuracy_parity(d32, d64, f64["par"], f64["cov"], f64["prior"], 32, "FP32 determinant")
+
+
+def test_count_nonfinite(p2r, torch):
+    cfg, trk, hit = helix(p2r, 1, 4)
+    trk = trk.copy()
+    trk.reshape(-1, 28, 32)[2, 3, 5] = np.inf  # 1/pT of one track
+    out = gpu_forward(p2r, torch, cfg, trk, hit)
+    assert p2r.count_nonfinite(dev(torch, out), cfg.nblocks, 32) == 1
+
+
+@pytest.mark.slow
+def test_full_size_chained_sample_vs_reference(p2r, oracle, torch):
+    """9600 tracks x 100 events x 20 layers on the GPU; 300 blocks checked against the reference."""
+    cfg, trk, hit = helix(p2r, 100, 300)
+    out = gpu_forward(p2r, torch, cfg, trk, hit)
+    assert np.isfinite(parity.unpack(out[: 600 * 28 * 32], 32)[0]).all()
+    dt = dev(torch, out)
+    assert p2r.count_nonfinite(dt, cfg.nblocks, 32) == 0
+    ref = ref_or_none(32, "kf")
+    if ref is None:
+        return
+    ref.set_bz(cfg.bz)
+    sel = np.random.default_rng(3).choice(cfg.nblocks, 300, replace=False)
+    t_s = np.ascontiguousarray(trk[sel])
+    h_s = np.ascontiguousarray(hit.reshape(cfg.nblocks, cfg.nlayer, 9, 32)[sel])
+    want = ref.run(t_s, h_s, 1, 300, cfg.nlayer, chained=True)
+    got = out.reshape(cfg.nblocks, 28, 32)[sel]
+    f64 = oracle.run(t_s, h_s, 32, cfg.nlayer, 1, cfg.bz, "f64")
+    parity.assert_accuracy_parity(got, want, f64["par"], f64["cov"], f64["prior"], 32, "full size sample")
