@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--mode", choices=["chained", "restart"], default="chained")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adj-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--ref-budget", type=float, default=90.0, help="reference arm: total seconds")
     return ap.parse_args()
@@ -302,6 +304,38 @@ def main():
     hbm_peak = peaks.get("hbm_gbs")
     traffic = traffic_from_profiles("chained")
 
+    # forward + adjoint (p2r_forward_backward: fused chained forward with checkpoints and
+    # the hand-written reverse sweep, plus the deterministic reduction of the shared
+    # gradients) against the plain fused forward, on the same workload
+    adjoint = None
+    if not args.no_adjoint:
+        g_trk = torch.randn(d_trk.numel(), dtype=torch.float32, device=dev, generator=torch.Generator(dev).manual_seed(1))
+        g_chi2 = torch.ones(cfg.ntracks, dtype=torch.float32, device=dev)
+        d_dr = torch.zeros(NLAYER, dtype=torch.float32, device=dev)
+        adjoint = {"ckpt_stride": {}, "steps": args.adj_steps}
+        ws = {}
+        for ck in (5, 1, 10):
+            for _ in range(2):
+                p2r.forward_backward(cfg, d_trk, d_hit, dr=d_dr, grad_trk_out=g_trk, grad_chi2=g_chi2,
+                                     ckpt_stride=ck, stream=stream, out=ws)
+            torch.cuda.synchronize()
+            barrier()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(args.adj_steps):
+                p2r.forward_backward(cfg, d_trk, d_hit, dr=d_dr, grad_trk_out=g_trk, grad_chi2=g_chi2,
+                                     ckpt_stride=ck, stream=stream, out=ws)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            ams = max_over_ranks(a0.elapsed_time(a1)) / args.adj_steps
+            adjoint["ckpt_stride"][str(ck)] = {"ms_per_step": ams, "ratio_vs_forward": ams / ms_per_step}
+        del ws
+        adjoint["ratio_vs_forward"] = adjoint["ckpt_stride"]["5"]["ratio_vs_forward"]
+        adjoint["definition"] = ("time of p2r_forward_backward (forward outputs + gradients w.r.t. initial "
+                                 "parameters/covariance, hits, per-layer dr and Bz of sum(g.out) + sum(chi2)) "
+                                 "divided by the plain p2r_forward time")
+
     # end to end through the host-buffer C-ABI call: H2D + kernels + D2H every step
     h_trk = torch.from_numpy(trk.reshape(-1)).pin_memory().numpy()
     h_hit = torch.from_numpy(hit.reshape(-1)).pin_memory().numpy()
@@ -356,6 +390,7 @@ def main():
                     "h2d_bytes_per_step": int(trk.nbytes + hit.nbytes), "d2h_bytes_per_step": int(trk.nbytes),
                     "steps": args.e2e_steps, "api": "p2r_forward_host (pinned host buffers, 10 chunks)",
                     "output_matches_device_run": bool(ok)},
+            "fwd_adjoint": adjoint,
             "gpu_launches": args.steps,
             "clocks": clk,
             "nonfinite_tracks": nonfinite,

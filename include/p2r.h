@@ -127,6 +127,33 @@ int p2r_count_nonfinite(const void* trk, int64_t nblocks, int32_t bsize, unsigne
 int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void* host_hits, void* host_trk_out,
                      void* dev_trk_in, void* dev_hits, void* dev_trk_out, int32_t nchunks, void* stream);
 
+/* ---------------------------------------------------------------- adjoint
+ * Fused forward + hand-written adjoint of the CHAINED layer loop (no counterpart in the
+ * reference, which has no derivatives). For the scalar
+ *   L = sum over tracks of  g_out . out  +  g_chi2 * chi2,
+ * out = the final parameters and covariance, chi2 = the summed chi2 of the track's updates
+ * (the reference's commented-out Chi2Similarity, TBB:631), it writes:
+ *   grad_trk_in   dL/d(initial par, cov)  (MPTRK layout, q row zero)       nullable
+ *   grad_hits     dL/d(hit pos, hit cov)  (MPHIT layout, every layer)      nullable
+ *   grad_dr       dL/d dr[layer], summed over tracks (nlayer doubles)     nullable
+ *   grad_bz       dL/d Bz, summed over tracks (1 double)                 nullable
+ *   grad_dr_event / grad_bz_event: the same per event ([nevts][nlayer], [nevts];
+ *                 needs bsize % 32 == 0)                                    nullable
+ * plus the forward outputs trk_out and chi2_out (nullable). grad_trk_out: cotangent of the
+ * final state (MPTRK layout, par and cov rows; nullable = 0); grad_chi2: one per track
+ * (nullable = 0). dr: radius offsets (nullable = 0); nlay_lane: per-track layer counts as
+ * in p2r_forward_masked (nullable). The state is stored every ckpt_stride layers (1, 2, 4,
+ * 5 or 10; 0 = 5) and the layers between checkpoints are recomputed. nlayer <= 64.
+ * workspace: device memory of p2r_forward_backward_workspace_size(cfg) bytes, 256-byte
+ * aligned (per-warp partial sums of the shared gradients, reduced in a fixed order in
+ * double, so results are deterministic). */
+size_t p2r_forward_backward_workspace_size(const p2r_config* cfg);
+int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* hits, const float* dr,
+                         const int32_t* nlay_lane, void* trk_out, float* chi2_out, const void* grad_trk_out,
+                         const float* grad_chi2, void* grad_trk_in, void* grad_hits, double* grad_dr,
+                         double* grad_bz, double* grad_dr_event, double* grad_bz_event, int32_t ckpt_stride,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- measurement helper
  * FP32 FMA throughput probe (the denominator of the FP32 compute roofline): blocks x
  * threads threads each run 8 independent FMA chains for 4*iters rounds; FLOPs per launch

@@ -47,10 +47,15 @@ struct Hit {
 template <class T>
 inline T hypot2(T x, T y) { return std::sqrt(x * x + y * y); }  // TBB:428-431
 
+// TBB:644-652 (4th-order cos, 3rd-order sin). omc = 1 - c is evaluated as x^2/2 - x^4/24,
+// the algebraically identical form the reference's -ffast-math build computes for its
+// 1 - cosa (TBB:738-739, 756, 763); formed as 1 - c in float it cancels for the tiny
+// angles of the later helix iterations.
 template <class T>
-inline void sincos4_(T x, T& s, T& c) {  // TBB:644-652 (4th-order cos, 3rd-order sin)
+inline void sincos4_(T x, T& s, T& c, T& omc) {
   const T x2 = x * x;
-  c = T(1) - T(0.5) * x2 + T(0.04166667f) * x2 * x2;
+  omc = T(0.5) * x2 - T(0.04166667f) * x2 * x2;
+  c = T(1) - omc;
   s = x - T(0.16666667f) * x * x2;
 }
 
@@ -66,7 +71,7 @@ void propagate_to_r(const Trk<T>& in, const T* hitpos, T dr, T kfact, Trk<T>& ou
   const T kinv = T(1) / k;
   const T pt = T(1) / iptin;
 
-  T D = 0, cosa = 0, sina = 0, id = 0;
+  T D = 0, cosa = 0, sina = 0, id = 0, omc = 0;
   const T cosP = std::cos(phiin), sinP = std::sin(phiin);
   T px = cosP * pt, py = sinP * pt;
   T dDdx = r0 > T(0) ? -xin / r0 : T(0);
@@ -79,7 +84,7 @@ void propagate_to_r(const Trk<T>& in, const T* hitpos, T dr, T kfact, Trk<T>& ou
     r0 = hypot2(xo, yo);
     id = r - r0;
     D += id;
-    sincos4_(id * iptin * kinv, sina, cosa);
+    sincos4_(id * iptin * kinv, sina, cosa, omc);
     if (i + 1 != niter) {
       // derivatives of the total path w.r.t. x, y, ipt, phi, only once the step is
       // below 1 um (TBB:714); the branch is part of the algorithm.
@@ -97,8 +102,8 @@ void propagate_to_r(const Trk<T>& in, const T* hitpos, T dr, T kfact, Trk<T>& ou
                      yo * (pyca * tmp + pxsa * tmp - pysa + pxca - px)) * pt * oor0;
       dDdphi += k * (xo * (pysa - px + pxca) - yo * (pxsa - py + pyca)) * oor0;
     }
-    xo = xo + k * (px * sina - py * (T(1) - cosa));
-    yo = yo + k * (py * sina + px * (T(1) - cosa));
+    xo = xo + k * (px * sina - py * omc);
+    yo = yo + k * (py * sina + px * omc);
     const T pxold = px;
     px = px * cosa - py * sina;
     py = py * cosa + pxold * sina;
@@ -109,17 +114,17 @@ void propagate_to_r(const Trk<T>& in, const T* hitpos, T dr, T kfact, Trk<T>& ou
   const T dady = dDdy * iptin * kinv;
   const T dadipt = (iptin * dDdipt + D) * kinv;
   const T dadphi = dDdphi * iptin * kinv;
-  sincos4_(alpha, sina, cosa);
+  sincos4_(alpha, sina, cosa, omc);
 
   // Transport Jacobian, dense 6x6 (TBB:753-807).
   T J[6][6] = {};
   J[0][0] = T(1) + k * dadx * (cosP * cosa - sinP * sina) * pt;
   J[0][1] = k * dady * (cosP * cosa - sinP * sina) * pt;
-  J[0][3] = k * (cosP * (iptin * dadipt * cosa - sina) + sinP * ((T(1) - cosa) - iptin * dadipt * sina)) * pt * pt;
+  J[0][3] = k * (cosP * (iptin * dadipt * cosa - sina) + sinP * (omc - iptin * dadipt * sina)) * pt * pt;
   J[0][4] = k * (cosP * dadphi * cosa - sinP * dadphi * sina - sinP * sina + cosP * cosa - cosP) * pt;
   J[1][0] = k * dadx * (sinP * cosa + cosP * sina) * pt;
   J[1][1] = T(1) + k * dady * (sinP * cosa + cosP * sina) * pt;
-  J[1][3] = k * (sinP * (iptin * dadipt * cosa - sina) + cosP * (iptin * dadipt * sina - (T(1) - cosa))) * pt * pt;
+  J[1][3] = k * (sinP * (iptin * dadipt * cosa - sina) + cosP * (iptin * dadipt * sina - omc)) * pt * pt;
   J[1][4] = k * (sinP * dadphi * cosa + cosP * dadphi * sina + sinP * cosa + cosP * sina - sinP) * pt;
   const T cosT = std::cos(thetain);
   const T isinT = T(1) / std::sin(thetain);
@@ -232,8 +237,9 @@ void load_hit(const float* blk, int bs, int it, Hit<T>& h) {
 //   nlay_lane (nullable): per-track layer count; lanes stop updating after it.
 // Output: float path -> MPTRK layout into out_f (28*bsize words per block);
 //         both paths -> per-track par (6) and cov (21) in double into par_d / cov_d
-//         (nullable), the summed chi2 into chi2_d (nullable), and the covariance that
-//         entered the last update into prior_d (nullable, 21 per track).
+//         (nullable), the chi2 into chi2_d (nullable; chained: summed over layers,
+//         restart: of the last layer's update, the only one that reaches the output), and
+//         the covariance that entered the last update into prior_d (nullable, 21 per track).
 template <class T>
 void run_tracks(const float* trk, const float* hit, long nblocks, int bs, int nlayer, int mode,
                 float kfact_f, double kfact_d, const double* dr, const int* nlay_lane, float* out_f,
@@ -257,6 +263,8 @@ void run_tracks(const float* trk, const float* hit, long nblocks, int bs, int nl
           propagate_to_r(st, h.pos, drl, kfact, st);
         if (prior_d)  // covariance entering the last update (the scale its rounding acts on)
           for (int i = 0; i < 21; ++i) prior_d[(b * bs + it) * 21 + i] = double(st.cov[i]);
+        // restart: only the last layer's update survives, and so does only its chi2
+        if (mode == 0) chi2 = 0;
         chi2 += kalman_update(st, h);
       }
       const long tr = b * bs + it;

@@ -9,7 +9,10 @@ from .api import (Config, KalmanUpdate, REF_BZ, count_nonfinite, forward, forwar
                   generate_fixture,
                   generate_helix, kfact, propagateToR, run_layers, summary, tracks_cov, tracks_par, tracks_q)
 
+from .autograd import P2RChain, forward_backward, workspace_size
+
 __all__ = [
+    "P2RChain", "forward_backward", "workspace_size",
     "Config", "KalmanUpdate", "propagateToR", "run_layers", "forward", "forward_host", "fp32_fma_probe",
     "count_nonfinite", "kfact",
     "gen_params", "generate_helix", "generate_fixture", "summary", "tracks_par", "tracks_cov", "tracks_q",

@@ -89,6 +89,9 @@ SIGNATURES = {
     "p2r_count_nonfinite": (ctypes.c_int, [_vp, _i64, _i32, _vp, _vp]),
     "p2r_forward_host": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "p2r_fp32_fma_probe": (ctypes.c_int, [_i64, _i32, _i32, _vp, _vp]),
+    "p2r_forward_backward_workspace_size": (ctypes.c_size_t, [_cfgp]),
+    "p2r_forward_backward": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                            _vp, _vp, _i32, _vp, ctypes.c_size_t, _vp]),
     "p2r_gen_params_default": (None, [ctypes.POINTER(CGenParams)]),
     "p2r_gen_helix": (ctypes.c_int, [ctypes.POINTER(CGenParams), _i32, _i64, _i64, _i32, _vp, _vp, _vp, _i32]),
     "p2r_gen_fixture": (ctypes.c_int, [_vp, _vp, _i32, _vp, _i32, _i32, _i64, _i64, _i32, ctypes.c_double, _vp, _vp]),

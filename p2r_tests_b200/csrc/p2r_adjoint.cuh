@@ -1,0 +1,664 @@
+// Hand-written reverse-mode derivative (adjoint) of one layer of the p2r hot path:
+// propagateToR (TBB:656-812) followed by KalmanUpdate (TBB:433-642), plus the update's
+// chi2 = res^T inv(R) res. Templated on the scalar type and usable on host and device:
+// the device kernel instantiates it in float, a host unit test in double (checked against
+// central finite differences of the double forward in this same header).
+//
+// The forward formulas are the reference's (see p2r_math.cuh for the float production
+// forward); the derivatives are those of the implemented arithmetic: the five fixed
+// helix iterations, the 4th-order sincos4 polynomials and the 1 um convergence branch of
+// the path derivatives (TBB:714) held fixed at the primal point.
+//
+// Symmetric matrices are packed lower-triangle (TBB:46-54). The adjoint of a packed
+// covariance treats each packed element as one variable: an off-diagonal slot collects
+// the derivatives of both (i,j) and (j,i) uses.
+#pragma once
+
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define P2R_HD __host__ __device__ __forceinline__
+#else
+#define P2R_HD inline
+#endif
+
+namespace p2r {
+namespace adj {
+
+P2R_HD constexpr int S6(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
+
+P2R_HD float sqrt_(float x) { return sqrtf(x); }
+P2R_HD double sqrt_(double x) { return sqrt(x); }
+P2R_HD float abs_(float x) { return fabsf(x); }
+P2R_HD double abs_(double x) { return fabs(x); }
+P2R_HD void sincos_(float x, float* s, float* c) {
+#if defined(__CUDA_ARCH__)
+  sincosf(x, s, c);
+#else
+  *s = sinf(x);
+  *c = cosf(x);
+#endif
+}
+P2R_HD void sincos_(double x, double* s, double* c) {
+#if defined(__CUDA_ARCH__)
+  sincos(x, s, c);
+#else
+  *s = sin(x);
+  *c = cos(x);
+#endif
+}
+
+template <class T>
+P2R_HD T hipo(T x, T y) { return sqrt_(x * x + y * y); }
+
+// sincos4 (TBB:644-652) with omc = 1 - c formed without cancellation, and its derivative
+template <class T>
+P2R_HD void sincos4(T x, T& s, T& c, T& omc) {
+  const T x2 = x * x;
+  omc = T(0.5f) * x2 - T(0.04166667f) * x2 * x2;
+  c = T(1) - omc;
+  s = x - T(0.16666667f) * x * x2;
+}
+template <class T>
+P2R_HD T sincos4_bar(T x, T sbar, T cbar) {
+  return cbar * (-x + T(4) * T(0.04166667f) * x * x * x) + sbar * (T(1) - T(3) * T(0.16666667f) * x * x);
+}
+
+// Forward values of one propagateToR that its reverse needs.
+template <class T>
+struct PropTape {
+  T r00, pt, cP, sP;
+  T xo[5], yo[5], px[5], py[5], r0[5];  // at the start of each helix iteration
+  T D, dDdx, dDdy, dDdipt, dDdphi;
+  T alpha, dadx, dady, dadipt, dadphi, sa, ca, omc, cT, sT, isT;
+  T J00, J01, J03, J04, J10, J11, J13, J14, J20, J21, J23, J24, J25, J40, J41, J43, J44;
+  T T0[6], T1[6], T2[6], T4[6];  // rows 0, 1, 2, 4 of J*C
+};
+
+// propagateToR of (ip, ic) to radius r with k = q*kfact, kinv = 1/k, recording the tape.
+template <class T>
+P2R_HD void prop_fwd(const T (&ip)[6], const T (&ic)[21], T k, T kinv, T r, PropTape<T>& t, T (&op)[6],
+                     T (&oc)[21]) {
+  const T xin = ip[0], yin = ip[1], zin = ip[2], iptin = ip[3], phiin = ip[4], thetain = ip[5];
+  t.r00 = hipo(xin, yin);
+  t.pt = T(1) / iptin;
+  sincos_(phiin, &t.sP, &t.cP);
+  T px = t.cP * t.pt, py = t.sP * t.pt;
+  T dDdx = t.r00 > T(0) ? -xin / t.r00 : T(0);
+  T dDdy = t.r00 > T(0) ? -yin / t.r00 : T(0);
+  T dDdipt = 0, dDdphi = 0, D = 0, sina, cosa, omc;
+  T xo = xin, yo = yin;
+  const T pt = t.pt;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    t.xo[i] = xo;
+    t.yo[i] = yo;
+    t.px[i] = px;
+    t.py[i] = py;
+    const T r0 = hipo(xo, yo);
+    t.r0[i] = r0;
+    const T id = r - r0;
+    D += id;
+    sincos4(id * iptin * kinv, sina, cosa, omc);
+    if (i + 1 != 5) {
+      const T oor0 = (r0 > T(0) && abs_(r - r0) < T(0.0001f)) ? T(1) / r0 : T(0);
+      const T dadipt = id * kinv;
+      const T dadx = -xo * iptin * kinv * oor0;
+      const T dady = -yo * iptin * kinv * oor0;
+      const T pxca = px * cosa, pxsa = px * sina, pyca = py * cosa, pysa = py * sina;
+      T tmp = k * dadx;
+      dDdx -= (xo * (T(1) + tmp * (pxca - pysa)) + yo * tmp * (pyca + pxsa)) * oor0;
+      tmp = k * dady;
+      dDdy -= (xo * tmp * (pxca - pysa) + yo * (T(1) + tmp * (pyca + pxsa))) * oor0;
+      tmp = dadipt * iptin;
+      dDdipt -= k * (xo * (pxca * tmp - pysa * tmp - pyca - pxsa + py) +
+                     yo * (pyca * tmp + pxsa * tmp - pysa + pxca - px)) * pt * oor0;
+      dDdphi += k * (xo * (pysa - px + pxca) - yo * (pxsa - py + pyca)) * oor0;
+    }
+    xo = xo + k * (px * sina - py * omc);
+    yo = yo + k * (py * sina + px * omc);
+    const T pxold = px;
+    px = px * cosa - py * sina;
+    py = py * cosa + pxold * sina;
+  }
+  t.D = D;
+  t.dDdx = dDdx;
+  t.dDdy = dDdy;
+  t.dDdipt = dDdipt;
+  t.dDdphi = dDdphi;
+  t.alpha = D * iptin * kinv;
+  t.dadx = dDdx * iptin * kinv;
+  t.dady = dDdy * iptin * kinv;
+  t.dadipt = (iptin * dDdipt + D) * kinv;
+  t.dadphi = dDdphi * iptin * kinv;
+  sincos4(t.alpha, t.sa, t.ca, t.omc);
+  const T cP = t.cP, sP = t.sP, ca = t.ca, sa = t.sa, alpha = t.alpha;
+  const T dadx = t.dadx, dady = t.dady, dadipt = t.dadipt, dadphi = t.dadphi;
+  t.J00 = T(1) + k * dadx * (cP * ca - sP * sa) * pt;
+  t.J01 = k * dady * (cP * ca - sP * sa) * pt;
+  t.J03 = k * (cP * (iptin * dadipt * ca - sa) + sP * (t.omc - iptin * dadipt * sa)) * pt * pt;
+  t.J04 = k * (cP * dadphi * ca - sP * dadphi * sa - sP * sa + cP * ca - cP) * pt;
+  t.J10 = k * dadx * (sP * ca + cP * sa) * pt;
+  t.J11 = T(1) + k * dady * (sP * ca + cP * sa) * pt;
+  t.J13 = k * (sP * (iptin * dadipt * ca - sa) + cP * (iptin * dadipt * sa - t.omc)) * pt * pt;
+  t.J14 = k * (sP * dadphi * ca + cP * dadphi * sa + sP * ca + cP * sa - sP) * pt;
+  sincos_(thetain, &t.sT, &t.cT);
+  t.isT = T(1) / t.sT;
+  const T cT = t.cT, isT = t.isT;
+  t.J20 = k * cT * dadx * pt * isT;
+  t.J21 = k * cT * dady * pt * isT;
+  t.J23 = k * cT * (iptin * dadipt - alpha) * pt * pt * isT;
+  t.J24 = k * dadphi * cT * pt * isT;
+  t.J25 = -k * alpha * pt * isT * isT;
+  t.J40 = dadx;
+  t.J41 = dady;
+  t.J43 = dadipt;
+  t.J44 = T(1) + dadphi;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const T c0 = ic[S6(0, j)], c1 = ic[S6(1, j)], c2 = ic[S6(2, j)], c3 = ic[S6(3, j)], c4 = ic[S6(4, j)],
+            c5 = ic[S6(5, j)];
+    t.T0[j] = t.J00 * c0 + t.J01 * c1 + t.J03 * c3 + t.J04 * c4;
+    t.T1[j] = t.J10 * c0 + t.J11 * c1 + t.J13 * c3 + t.J14 * c4;
+    t.T2[j] = t.J20 * c0 + t.J21 * c1 + c2 + t.J23 * c3 + t.J24 * c4 + t.J25 * c5;
+    t.T4[j] = t.J40 * c0 + t.J41 * c1 + t.J43 * c3 + t.J44 * c4;
+  }
+  // C' = (J C) J^T, lower triangle; rows 3 and 5 of J C are rows 3 and 5 of C
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    T Ti[6];
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+      Ti[j] = i == 0 ? t.T0[j] : i == 1 ? t.T1[j] : i == 2 ? t.T2[j] : i == 4 ? t.T4[j] : ic[S6(i, j)];
+    oc[S6(i, 0)] = Ti[0] * t.J00 + Ti[1] * t.J01 + Ti[3] * t.J03 + Ti[4] * t.J04;
+    if (i >= 1) oc[S6(i, 1)] = Ti[0] * t.J10 + Ti[1] * t.J11 + Ti[3] * t.J13 + Ti[4] * t.J14;
+    if (i >= 2)
+      oc[S6(i, 2)] = Ti[0] * t.J20 + Ti[1] * t.J21 + Ti[2] + Ti[3] * t.J23 + Ti[4] * t.J24 + Ti[5] * t.J25;
+    if (i >= 3) oc[S6(i, 3)] = Ti[3];
+    if (i >= 4) oc[S6(i, 4)] = Ti[0] * t.J40 + Ti[1] * t.J41 + Ti[3] * t.J43 + Ti[4] * t.J44;
+    if (i >= 5) oc[S6(i, 5)] = Ti[5];
+  }
+  op[0] = xo;
+  op[1] = yo;
+  op[2] = zin + k * alpha * cT * pt * isT;
+  op[3] = iptin;
+  op[4] = phiin + alpha;
+  op[5] = thetain;
+}
+
+// Reverse of prop_fwd. In: the tape, the input (ip, ic), adjoints pb_out / cb_out of the
+// outputs. Out: adjoints pb_in / cb_in of the inputs (overwritten); rbar, kbar and kinvbar
+// are accumulated (+=).
+template <class T>
+P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], T k, T kinv, T r,
+                     const T (&pb_out)[6], const T (&cb_out)[21], T (&pb_in)[6], T (&cb_in)[21], T& rbar, T& kbar,
+                     T& kinvbar) {
+  const T x = ip[0], y = ip[1], ipt = ip[3];
+  const T pt = t.pt, cP = t.cP, sP = t.sP, ca = t.ca, sa = t.sa, cT = t.cT, sT = t.sT, isT = t.isT;
+  const T alpha = t.alpha, dadx = t.dadx, dady = t.dady, dadipt = t.dadipt, dadphi = t.dadphi;
+
+  T xob = pb_out[0], yob = pb_out[1];
+  const T zb = pb_out[2];
+  T iptb = pb_out[3], phib = pb_out[4], alphab = pb_out[4], thetab = pb_out[5];
+  // z' = z + k*alpha*cT*pt*isT
+  kbar += zb * alpha * cT * pt * isT;
+  alphab += zb * k * cT * pt * isT;
+  T cTb = zb * k * alpha * pt * isT;
+  T ptb = zb * k * alpha * cT * isT;
+  T isTb = zb * k * alpha * cT * pt;
+
+  // ---- C' = J C J^T: S = Gbar + Gbar^T, Jbar = S (J C), cbar = packed(J^T S J)
+  T S[6][6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) S[i][j] = i == j ? T(2) * cb_out[S6(i, i)] : cb_out[S6(i, j)];
+  T Tf[6][6];
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    Tf[0][j] = t.T0[j];
+    Tf[1][j] = t.T1[j];
+    Tf[2][j] = t.T2[j];
+    Tf[3][j] = ic[S6(3, j)];
+    Tf[4][j] = t.T4[j];
+    Tf[5][j] = ic[S6(5, j)];
+  }
+  auto ST = [&](int a, int b) {
+    T s = 0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) s += S[a][c] * Tf[c][b];
+    return s;
+  };
+  const T J00b = ST(0, 0), J01b = ST(0, 1), J03b = ST(0, 3), J04b = ST(0, 4);
+  const T J10b = ST(1, 0), J11b = ST(1, 1), J13b = ST(1, 3), J14b = ST(1, 4);
+  const T J20b = ST(2, 0), J21b = ST(2, 1), J23b = ST(2, 3), J24b = ST(2, 4), J25b = ST(2, 5);
+  const T J40b = ST(4, 0), J41b = ST(4, 1), J43b = ST(4, 3), J44b = ST(4, 4);
+  // W = S J, M = J^T W
+  T W[6][6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    W[a][0] = S[a][0] * t.J00 + S[a][1] * t.J10 + S[a][2] * t.J20 + S[a][4] * t.J40;
+    W[a][1] = S[a][0] * t.J01 + S[a][1] * t.J11 + S[a][2] * t.J21 + S[a][4] * t.J41;
+    W[a][2] = S[a][2];
+    W[a][3] = S[a][0] * t.J03 + S[a][1] * t.J13 + S[a][2] * t.J23 + S[a][3] + S[a][4] * t.J43;
+    W[a][4] = S[a][0] * t.J04 + S[a][1] * t.J14 + S[a][2] * t.J24 + S[a][4] * t.J44;
+    W[a][5] = S[a][2] * t.J25 + S[a][5];
+  }
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    T M[6];
+    M[0] = t.J00 * W[0][j] + t.J10 * W[1][j] + t.J20 * W[2][j] + t.J40 * W[4][j];
+    M[1] = t.J01 * W[0][j] + t.J11 * W[1][j] + t.J21 * W[2][j] + t.J41 * W[4][j];
+    M[2] = W[2][j];
+    M[3] = t.J03 * W[0][j] + t.J13 * W[1][j] + t.J23 * W[2][j] + W[3][j] + t.J43 * W[4][j];
+    M[4] = t.J04 * W[0][j] + t.J14 * W[1][j] + t.J24 * W[2][j] + t.J44 * W[4][j];
+    M[5] = t.J25 * W[2][j] + W[5][j];
+#pragma unroll
+    for (int i = j; i < 6; ++i) cb_in[S6(i, j)] = i == j ? T(0.5f) * M[i] : M[i];
+  }
+
+  // ---- Jacobian entries -> their inputs
+  const T U = cP * ca - sP * sa, V = sP * ca + cP * sa, w = ipt * dadipt;
+  T Ub = 0, Vb = 0, wb = 0, dadxb = 0, dadyb = 0, dadiptb = 0, dadphib = 0, cPb = 0, sPb = 0;
+  kbar += J00b * dadx * U * pt;
+  dadxb += J00b * k * U * pt;
+  Ub += J00b * k * dadx * pt;
+  ptb += J00b * k * dadx * U;
+  kbar += J01b * dady * U * pt;
+  dadyb += J01b * k * U * pt;
+  Ub += J01b * k * dady * pt;
+  ptb += J01b * k * dady * U;
+  {
+    const T Q = w * U - V + sP, g = J03b * k * pt * pt;
+    kbar += J03b * pt * pt * Q;
+    ptb += J03b * T(2) * k * pt * Q;
+    wb += g * U;
+    Ub += g * w;
+    Vb -= g;
+    sPb += g;
+  }
+  {
+    const T Q = (dadphi + T(1)) * U - cP, g = J04b * k * pt;
+    kbar += J04b * pt * Q;
+    ptb += J04b * k * Q;
+    dadphib += g * U;
+    Ub += g * (dadphi + T(1));
+    cPb -= g;
+  }
+  kbar += J10b * dadx * V * pt;
+  dadxb += J10b * k * V * pt;
+  Vb += J10b * k * dadx * pt;
+  ptb += J10b * k * dadx * V;
+  kbar += J11b * dady * V * pt;
+  dadyb += J11b * k * V * pt;
+  Vb += J11b * k * dady * pt;
+  ptb += J11b * k * dady * V;
+  {
+    const T Q = w * V + U - cP, g = J13b * k * pt * pt;
+    kbar += J13b * pt * pt * Q;
+    ptb += J13b * T(2) * k * pt * Q;
+    wb += g * V;
+    Vb += g * w;
+    Ub += g;
+    cPb -= g;
+  }
+  {
+    const T Q = (dadphi + T(1)) * V - sP, g = J14b * k * pt;
+    kbar += J14b * pt * Q;
+    ptb += J14b * k * Q;
+    dadphib += g * V;
+    Vb += g * (dadphi + T(1));
+    sPb -= g;
+  }
+  {
+    const T G = k * cT * pt * isT;
+    const T Gb = J20b * dadx + J21b * dady + J23b * pt * (w - alpha) + J24b * dadphi;
+    dadxb += J20b * G;
+    dadyb += J21b * G;
+    ptb += J23b * G * (w - alpha);
+    wb += J23b * G * pt;
+    alphab -= J23b * G * pt;
+    dadphib += J24b * G;
+    kbar += Gb * cT * pt * isT;
+    cTb += Gb * k * pt * isT;
+    ptb += Gb * k * cT * isT;
+    isTb += Gb * k * cT * pt;
+  }
+  kbar -= J25b * alpha * pt * isT * isT;
+  alphab -= J25b * k * pt * isT * isT;
+  ptb -= J25b * k * alpha * isT * isT;
+  isTb -= J25b * T(2) * k * alpha * pt * isT;
+  dadxb += J40b;
+  dadyb += J41b;
+  dadiptb += J43b;
+  dadphib += J44b;
+  iptb += wb * dadipt;
+  dadiptb += wb * ipt;
+  cPb += Ub * ca + Vb * sa;
+  sPb += -Ub * sa + Vb * ca;
+  const T cab = Ub * cP + Vb * sP;
+  const T sab = -Ub * sP + Vb * cP;
+  alphab += sincos4_bar(alpha, sab, cab);
+  thetab += -cTb * sT - isTb * cT * isT * isT;
+
+  // ---- alpha, dad* from D and the path derivatives
+  T Db = alphab * ipt * kinv + dadiptb * kinv;
+  iptb += alphab * t.D * kinv + dadxb * t.dDdx * kinv + dadyb * t.dDdy * kinv + dadiptb * t.dDdipt * kinv +
+          dadphib * t.dDdphi * kinv;
+  kinvbar += alphab * t.D * ipt + dadxb * t.dDdx * ipt + dadyb * t.dDdy * ipt + dadiptb * (ipt * t.dDdipt + t.D) +
+             dadphib * t.dDdphi * ipt;
+  const T dDdxb = dadxb * ipt * kinv, dDdyb = dadyb * ipt * kinv;
+  const T dDdiptb = dadiptb * ipt * kinv, dDdphib = dadphib * ipt * kinv;
+
+  // ---- the five helix iterations, last to first
+  T pxb = 0, pyb = 0;
+#pragma unroll
+  for (int i = 4; i >= 0; --i) {
+    const T xo = t.xo[i], yo = t.yo[i], px = t.px[i], py = t.py[i], r0 = t.r0[i];
+    const T id = r - r0;
+    const T a = id * ipt * kinv;
+    T sai, cai, omci;
+    sincos4(a, sai, cai, omci);
+    // xo' = xo + k(px sa - py(1-ca)), yo' = yo + k(py sa + px(1-ca)),
+    // px' = px ca - py sa, py' = py ca + px sa
+    T sab_i = xob * k * px + yob * k * py - pxb * py + pyb * px;
+    T cab_i = xob * k * py - yob * k * px + pxb * px + pyb * py;
+    kbar += xob * (px * sai - py * omci) + yob * (py * sai + px * omci);
+    const T pxb_n = xob * k * sai + yob * k * omci + pxb * cai + pyb * sai;
+    const T pyb_n = -xob * k * omci + yob * k * sai - pxb * sai + pyb * cai;
+    pxb = pxb_n;
+    pyb = pyb_n;
+    T idb = Db;
+    T r0b = 0;
+    if (i < 4) {
+      const T o = (r0 > T(0) && abs_(r - r0) < T(0.0001f)) ? T(1) / r0 : T(0);
+      if (o != T(0)) {
+        const T dxb = -dDdxb, dyb = -dDdyb, dib = -dDdiptb, dpb = dDdphib;  // adjoints of the increments
+        const T dadipt_i = id * kinv, dadx_i = -xo * ipt * kinv * o, dady_i = -yo * ipt * kinv * o;
+        const T pxca = px * cai, pxsa = px * sai, pyca = py * cai, pysa = py * sai;
+        const T m1 = pxca - pysa, m2 = pyca + pxsa;
+        const T t1 = k * dadx_i, t2 = k * dady_i, t3 = dadipt_i * ipt;
+        T ob = 0, m1b = 0, m2b = 0;
+        // inc_x = (xo (1 + t1 m1) + yo t1 m2) o
+        xob += dxb * (T(1) + t1 * m1) * o;
+        yob += dxb * t1 * m2 * o;
+        const T t1b = dxb * (xo * m1 + yo * m2) * o;
+        m1b += dxb * xo * t1 * o;
+        m2b += dxb * yo * t1 * o;
+        ob += dxb * (xo * (T(1) + t1 * m1) + yo * t1 * m2);
+        // inc_y = (xo t2 m1 + yo (1 + t2 m2)) o
+        xob += dyb * t2 * m1 * o;
+        yob += dyb * (T(1) + t2 * m2) * o;
+        const T t2b = dyb * (xo * m1 + yo * m2) * o;
+        m1b += dyb * xo * t2 * o;
+        m2b += dyb * yo * t2 * o;
+        ob += dyb * (xo * t2 * m1 + yo * (T(1) + t2 * m2));
+        // inc_ipt = k Q pt o, Q = xo (m1 t3 - m2 + py) + yo (m2 t3 + m1 - px)
+        const T Q = xo * (m1 * t3 - m2 + py) + yo * (m2 * t3 + m1 - px);
+        kbar += dib * Q * pt * o;
+        ptb += dib * k * Q * o;
+        ob += dib * k * Q * pt;
+        const T Qb = dib * k * pt * o;
+        xob += Qb * (m1 * t3 - m2 + py);
+        yob += Qb * (m2 * t3 + m1 - px);
+        m1b += Qb * (xo * t3 + yo);
+        m2b += Qb * (-xo + yo * t3);
+        const T t3b = Qb * (xo * m1 + yo * m2);
+        pyb += Qb * xo;
+        pxb -= Qb * yo;
+        // inc_phi = k P o, P = xo n1 - yo n2, n1 = py sa + px ca - px, n2 = px sa + py ca - py
+        const T n1 = pysa + pxca - px, n2 = pxsa + pyca - py;
+        const T P = xo * n1 - yo * n2;
+        kbar += dpb * P * o;
+        ob += dpb * k * P;
+        const T Pb = dpb * k * o;
+        xob += Pb * n1;
+        yob -= Pb * n2;
+        const T n1b = Pb * xo, n2b = -Pb * yo;
+        pyb += n1b * sai;
+        sab_i += n1b * py;
+        pxb += n1b * (cai - T(1));
+        cab_i += n1b * px;
+        pxb += n2b * sai;
+        sab_i += n2b * px;
+        pyb += n2b * (cai - T(1));
+        cab_i += n2b * py;
+        // m1 = px ca - py sa, m2 = py ca + px sa
+        pxb += m1b * cai + m2b * sai;
+        pyb += -m1b * sai + m2b * cai;
+        cab_i += m1b * px + m2b * py;
+        sab_i += -m1b * py + m2b * px;
+        // t1 = k dadx_i, t2 = k dady_i, t3 = dadipt_i ipt
+        kbar += t1b * dadx_i + t2b * dady_i;
+        const T dadxib = t1b * k, dadyib = t2b * k, dadiptib = t3b * ipt;
+        iptb += t3b * dadipt_i;
+        xob -= dadxib * ipt * kinv * o;
+        iptb -= dadxib * xo * kinv * o;
+        kinvbar -= dadxib * xo * ipt * o;
+        ob -= dadxib * xo * ipt * kinv;
+        yob -= dadyib * ipt * kinv * o;
+        iptb -= dadyib * yo * kinv * o;
+        kinvbar -= dadyib * yo * ipt * o;
+        ob -= dadyib * yo * ipt * kinv;
+        idb += dadiptib * kinv;
+        kinvbar += dadiptib * id;
+        r0b -= ob * o * o;
+      }
+    }
+    const T ab = sincos4_bar(a, sab_i, cab_i);
+    idb += ab * ipt * kinv;
+    iptb += ab * id * kinv;
+    kinvbar += ab * id * ipt;
+    rbar += idb;
+    r0b -= idb;
+    if (r0 > T(0)) {
+      xob += r0b * xo / r0;
+      yob += r0b * yo / r0;
+    }
+  }
+  // ---- initial values: dDdx0 = -x/r00, dDdy0 = -y/r00 (r00 > 0), px0 = cP pt, py0 = sP pt
+  if (t.r00 > T(0)) {
+    const T r00 = t.r00;
+    const T r00b = (dDdxb * x + dDdyb * y) / (r00 * r00);
+    xob += -dDdxb / r00 + r00b * x / r00;
+    yob += -dDdyb / r00 + r00b * y / r00;
+  }
+  cPb += pxb * pt;
+  sPb += pyb * pt;
+  ptb += pxb * cP + pyb * sP;
+  phib += -cPb * sP + sPb * cP;
+  iptb -= ptb * pt * pt;
+  pb_in[0] = xob;
+  pb_in[1] = yob;
+  pb_in[2] = zb;
+  pb_in[3] = iptb;
+  pb_in[4] = phib;
+  pb_in[5] = thetab;
+}
+
+// KalmanUpdate of (p, c) with hit (hp, hc), forward in the reference's operation order
+// (TBB:433-642); returns chi2. The determinant is taken in double (TBB:457).
+template <class T>
+P2R_HD T upd_fwd(T (&p)[6], T (&c)[21], const T (&hp)[3], const T (&hc)[6]) {
+  const T rh = hipo(hp[0], hp[1]);
+  const T R00 = -(hp[1] + p[1]) / (T(2) * rh);
+  const T R01 = (hp[0] + p[0]) / (T(2) * rh);
+  const T e0 = (R00 * (c[0] + hc[0]) + R01 * (c[1] + hc[1])) * R00 + (R00 * (c[1] + hc[1]) + R01 * (c[2] + hc[2])) * R01;
+  const T e1 = (c[3] + hc[3]) * R00 + (c[4] + hc[4]) * R01;
+  const T e2 = c[5] + hc[5];
+  const double det = (double)e0 * e2 - (double)e1 * e1;
+  const T s = T(1.0 / det);
+  const T i0 = s * e2, i1 = e1 * -s, i2 = s * e0;
+  T K0[6], K1[6];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const T cm0 = c[S6(m, 0)], cm1 = c[S6(m, 1)], cm2 = c[S6(m, 2)];
+    K0[m] = cm0 * (R00 * i0) + cm1 * (R01 * i0) + cm2 * i1;
+    K1[m] = cm0 * (R00 * i1) + cm1 * (R01 * i1) + cm2 * i2;
+  }
+  const T res0 = R00 * (hp[0] - p[0]) + R01 * (hp[1] - p[1]);
+  const T res1 = hp[2] - p[2];
+  const T chi2 = i0 * res0 * res0 + T(2) * i1 * res0 * res1 + i2 * res1 * res1;
+#pragma unroll
+  for (int m = 0; m < 6; ++m) p[m] = p[m] + K0[m] * res0 + K1[m] * res1;
+  T nc[21];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = 0; j <= i; ++j)
+      nc[S6(i, j)] = c[S6(i, j)] - (K0[i] * R00 * c[S6(0, j)] + K0[i] * R01 * c[S6(1, j)] + K1[i] * c[S6(2, j)]);
+#pragma unroll
+  for (int i = 0; i < 21; ++i) c[i] = nc[i];
+  return chi2;
+}
+
+// Reverse of upd_fwd at the input (p, c, hp, hc). pb / cb: in = adjoints of the updated
+// state, out = adjoints of the state before the update (overwritten in place).
+// chi2b: adjoint of the update's chi2. hpb / hcb: adjoints of the hit (overwritten).
+template <class T>
+P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T (&hc)[6], T (&pb)[6], T (&cb)[21],
+                    T chi2b, T (&hpb)[3], T (&hcb)[6]) {
+  const T rh = hipo(hp[0], hp[1]);
+  const T den = T(2) * rh;
+  const T R00 = -(hp[1] + p[1]) / den, R01 = (hp[0] + p[0]) / den;
+  T A[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) A[k] = c[k] + hc[k];
+  const T e0 = R00 * R00 * A[0] + T(2) * R00 * R01 * A[1] + R01 * R01 * A[2];
+  const T e1 = A[3] * R00 + A[4] * R01, e2 = A[5];
+  const T s = T(1) / (e0 * e2 - e1 * e1);
+  const T i0 = s * e2, i1 = -s * e1, i2 = s * e0;
+  T B0[6], B1[6], K0[6], K1[6];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    B0[m] = R00 * c[S6(m, 0)] + R01 * c[S6(m, 1)];
+    B1[m] = c[S6(m, 2)];
+    K0[m] = B0[m] * i0 + B1[m] * i1;
+    K1[m] = B0[m] * i1 + B1[m] * i2;
+  }
+  const T res0 = R00 * (hp[0] - p[0]) + R01 * (hp[1] - p[1]), res1 = hp[2] - p[2];
+
+  // C' = C - K0 B0^T - K1 B1^T (lower triangle); p' = p + K0 res0 + K1 res1
+  T K0b[6], K1b[6], B0b[6], B1b[6];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    T a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+#pragma unroll
+    for (int j = 0; j <= m; ++j) {
+      a0 += cb[S6(m, j)] * B0[j];
+      a1 += cb[S6(m, j)] * B1[j];
+    }
+#pragma unroll
+    for (int i = m; i < 6; ++i) {
+      b0 += cb[S6(i, m)] * K0[i];
+      b1 += cb[S6(i, m)] * K1[i];
+    }
+    K0b[m] = -a0 + pb[m] * res0;
+    K1b[m] = -a1 + pb[m] * res1;
+    B0b[m] = -b0;
+    B1b[m] = -b1;
+  }
+  T res0b = 0, res1b = 0;
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    res0b += pb[m] * K0[m];
+    res1b += pb[m] * K1[m];
+  }
+  // chi2 = i0 res0^2 + 2 i1 res0 res1 + i2 res1^2
+  T i0b = chi2b * res0 * res0, i1b = chi2b * T(2) * res0 * res1, i2b = chi2b * res1 * res1;
+  res0b += chi2b * (T(2) * i0 * res0 + T(2) * i1 * res1);
+  res1b += chi2b * (T(2) * i1 * res0 + T(2) * i2 * res1);
+  // K0 = B0 i0 + B1 i1, K1 = B0 i1 + B1 i2
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    i0b += K0b[m] * B0[m];
+    i1b += K0b[m] * B1[m] + K1b[m] * B0[m];
+    i2b += K1b[m] * B1[m];
+    B0b[m] += K0b[m] * i0 + K1b[m] * i1;
+    B1b[m] += K0b[m] * i1 + K1b[m] * i2;
+  }
+  // B0_m = R00 C_m0 + R01 C_m1, B1_m = C_m2 (cb keeps the direct C' = C ... path)
+  T R00b = 0, R01b = 0;
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    R00b += B0b[m] * c[S6(m, 0)];
+    R01b += B0b[m] * c[S6(m, 1)];
+    cb[S6(m, 0)] += B0b[m] * R00;
+    cb[S6(m, 1)] += B0b[m] * R01;
+    cb[S6(m, 2)] += B1b[m];
+  }
+  // (i0, i1, i2) = (e2, -e1, e0) / det
+  T e2b = i0b * s, e1b = -i1b * s, e0b = i2b * s;
+  const T sb = i0b * e2 - i1b * e1 + i2b * e0;
+  const T detb = -sb * s * s;
+  e0b += detb * e2;
+  e2b += detb * e0;
+  e1b -= T(2) * detb * e1;
+  // residual
+  R00b += res0b * (hp[0] - p[0]);
+  R01b += res0b * (hp[1] - p[1]);
+  hpb[0] = res0b * R00;
+  hpb[1] = res0b * R01;
+  hpb[2] = res1b;
+  pb[0] -= res0b * R00;
+  pb[1] -= res0b * R01;
+  pb[2] -= res1b;
+  // e0 = R00^2 A0 + 2 R00 R01 A1 + R01^2 A2, e1 = A3 R00 + A4 R01, e2 = A5
+  R00b += e0b * (T(2) * R00 * A[0] + T(2) * R01 * A[1]) + e1b * A[3];
+  R01b += e0b * (T(2) * R00 * A[1] + T(2) * R01 * A[2]) + e1b * A[4];
+  hcb[0] = e0b * R00 * R00;
+  hcb[1] = e0b * T(2) * R00 * R01;
+  hcb[2] = e0b * R01 * R01;
+  hcb[3] = e1b * R00;
+  hcb[4] = e1b * R01;
+  hcb[5] = e2b;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) cb[k] += hcb[k];
+  // R00 = -(hy + y)/den, R01 = (hx + x)/den, den = 2 hipo(hx, hy)
+  hpb[1] -= R00b / den;
+  pb[1] -= R00b / den;
+  hpb[0] += R01b / den;
+  pb[0] += R01b / den;
+  const T rhb = T(2) * (-(R00b * R00 + R01b * R01) / den);
+  if (rh > T(0)) {
+    hpb[0] += rhb * hp[0] / rh;
+    hpb[1] += rhb * hp[1] / rh;
+  }
+}
+
+// One full layer, forward (state in place; returns chi2): propagate to hipo(hp) + dr, update.
+template <class T>
+P2R_HD T layer_fwd(T (&p)[6], T (&c)[21], T k, T kinv, const T (&hp)[3], const T (&hc)[6], T dr) {
+  PropTape<T> t;
+  const T r = hipo(hp[0], hp[1]) + dr;
+  prop_fwd(p, c, k, kinv, r, t, p, c);
+  return upd_fwd(p, c, hp, hc);
+}
+
+// Reverse of layer_fwd at the state (p, c) BEFORE the layer. pb / cb: in = adjoints of the
+// state after the layer, out = adjoints of the state before it. chi2b: adjoint of this
+// layer's chi2. hpb / hcb (overwritten), drb, kbar, kinvbar (accumulated).
+template <class T>
+P2R_HD void layer_rev(const T (&p)[6], const T (&c)[21], T k, T kinv, const T (&hp)[3], const T (&hc)[6], T dr,
+                      T (&pb)[6], T (&cb)[21], T chi2b, T (&hpb)[3], T (&hcb)[6], T& drb, T& kbar, T& kinvbar) {
+  PropTape<T> t;
+  const T rh = hipo(hp[0], hp[1]);
+  const T r = rh + dr;
+  T pp[6], pc[21];
+  prop_fwd(p, c, k, kinv, r, t, pp, pc);
+  upd_rev(pp, pc, hp, hc, pb, cb, chi2b, hpb, hcb);
+  T pin[6], cin[21], rbar = 0;
+  prop_rev(t, p, c, k, kinv, r, pb, cb, pin, cin, rbar, kbar, kinvbar);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) pb[i] = pin[i];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) cb[i] = cin[i];
+  drb += rbar;
+  if (rh > T(0)) {
+    hpb[0] += rbar * hp[0] / rh;
+    hpb[1] += rbar * hp[1] / rh;
+  }
+}
+
+}  // namespace adj
+}  // namespace p2r

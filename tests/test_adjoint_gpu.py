@@ -1,0 +1,173 @@
+"""GPU tests of the hand-written adjoint (p2r_forward_backward) through the C ABI.
+
+Reference gradient: torch autograd in FP64 over oracle/p2r_torch.py (pinned to the C
+oracle and to central finite differences in tests/test_adjoint_cpu.py). Tolerance: each
+gradient within 1e-3 relative of the FP64 reference, relative to max(|g|, 1e-3 * the
+largest |g| of that gradient group) so components that are zero to rounding are judged
+against the group's scale.
+"""
+import numpy as np
+import pytest
+
+from tests import parity
+
+pytestmark = pytest.mark.gpu
+
+GRAD_RTOL = 1e-3
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def setup(p2r, torch, nevts=1, nb=8, nlayer=20, seed=20240001):
+    cfg = p2r.Config(bsize=32, nlayer=nlayer, nevts=nevts, nb=nb, bz=3.8)
+    trk, hit = p2r.generate_helix(cfg, p2r.gen_params(bz=3.8, seed=seed))
+    rng = np.random.default_rng(seed)
+    dr = rng.uniform(-0.01, 0.01, nlayer).astype(np.float32)  # +-100 um
+    g_trk = np.zeros_like(trk)
+    g_trk[:, 0:6, :] = rng.normal(size=(cfg.nblocks, 6, 32))
+    g_trk[:, 6:27, :] = rng.normal(size=(cfg.nblocks, 21, 32)) * 1e2
+    g_chi2 = rng.uniform(0.5, 1.5, cfg.ntracks).astype(np.float32)
+    return cfg, trk, hit, dr, g_trk, g_chi2
+
+
+def torch_reference(p2r, cfg, trk, hit, dr, g_trk, g_chi2, nlay=None):
+    """FP64 reference gradients by torch autograd over the oracle restatement (CPU)."""
+    import torch as T
+    from oracle import p2r_torch
+    bs = cfg.bsize
+    t = trk.reshape(cfg.nblocks, 28, bs)
+    h = hit.reshape(cfg.nblocks, cfg.nlayer, 9, bs)
+    par0 = T.tensor(t[:, 0:6, :].transpose(0, 2, 1).reshape(-1, 6), dtype=T.float64, requires_grad=True)
+    cov0 = T.tensor(t[:, 6:27, :].transpose(0, 2, 1).reshape(-1, 21), dtype=T.float64, requires_grad=True)
+    q = T.tensor(p2r.tracks_q(t))
+    hpos = T.tensor(h[:, :, 0:3, :].transpose(0, 3, 1, 2).reshape(-1, cfg.nlayer, 3), dtype=T.float64,
+                    requires_grad=True)
+    hcov = T.tensor(h[:, :, 3:9, :].transpose(0, 3, 1, 2).reshape(-1, cfg.nlayer, 6), dtype=T.float64,
+                    requires_grad=True)
+    drt = T.tensor(dr.astype(np.float64), requires_grad=True)
+    bz = T.tensor(cfg.bz, dtype=T.float64, requires_grad=True)
+    nl = None if nlay is None else T.tensor(nlay)
+    par, cov, chi2 = p2r_torch.chained(par0, cov0, q, hpos, hcov, drt, bz, nl)
+    gt = g_trk.reshape(cfg.nblocks, 28, bs)
+    gp = T.tensor(gt[:, 0:6, :].transpose(0, 2, 1).reshape(-1, 6), dtype=T.float64)
+    gc = T.tensor(gt[:, 6:27, :].transpose(0, 2, 1).reshape(-1, 21), dtype=T.float64)
+    L = (gp * par).sum() + (gc * cov).sum() + (T.tensor(g_chi2, dtype=T.float64) * chi2).sum()
+    L.backward()
+    return dict(par0=par0.grad.numpy(), cov0=cov0.grad.numpy(), hpos=hpos.grad.numpy(), hcov=hcov.grad.numpy(),
+                dr=drt.grad.numpy(), bz=float(bz.grad), out_par=par.detach().numpy(), chi2=chi2.detach().numpy())
+
+
+def gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=5, nlay=None, per_event=False):
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
+    o = p2r.forward_backward(cfg, d(trk), d(hit), dr=d(dr), nlay_lane=None if nlay is None else d(nlay),
+                             grad_trk_out=d(g_trk), grad_chi2=d(g_chi2), ckpt_stride=ckpt, per_event=per_event)
+    torch.cuda.synchronize()
+    bs = cfg.bsize
+    gt = o["grad_trk_in"].cpu().numpy().reshape(cfg.nblocks, 28, bs)
+    gh = o["grad_hits"].cpu().numpy().reshape(cfg.nblocks, cfg.nlayer, 9, bs)
+    res = dict(par0=gt[:, 0:6, :].transpose(0, 2, 1).reshape(-1, 6),
+               cov0=gt[:, 6:27, :].transpose(0, 2, 1).reshape(-1, 21),
+               hpos=gh[:, :, 0:3, :].transpose(0, 3, 1, 2).reshape(-1, cfg.nlayer, 3),
+               hcov=gh[:, :, 3:9, :].transpose(0, 3, 1, 2).reshape(-1, cfg.nlayer, 6),
+               dr=o["grad_dr"].cpu().numpy(), bz=float(o["grad_bz"].cpu().numpy()[0]),
+               trk_out=o["trk_out"].cpu().numpy(), chi2=o["chi2"].cpu().numpy())
+    if per_event:
+        res["dr_event"] = o["grad_dr_event"].cpu().numpy()
+        res["bz_event"] = o["grad_bz_event"].cpu().numpy()
+    return res
+
+
+def grad_err(g, ref):
+    g, ref = np.asarray(g, np.float64), np.asarray(ref, np.float64)
+    scale = max(np.abs(ref).max(), 1e-300)
+    return np.abs(g - ref) / np.maximum(np.abs(ref), 1e-3 * scale)
+
+
+def test_adjoint_matches_fp64_reference(p2r, torch):
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch)
+    ref = torch_reference(p2r, cfg, trk, hit, dr, g_trk, g_chi2)
+    got = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2)
+    report = {}
+    for key in ("par0", "cov0", "hpos", "hcov", "dr"):
+        e = grad_err(got[key], ref[key])
+        report[key] = (float(np.quantile(e, 0.99)), float(e.max()))
+    report["bz"] = float(grad_err([got["bz"]], [ref["bz"]])[0])
+    for key in ("par0", "hpos", "dr"):
+        assert report[key][0] < GRAD_RTOL, report
+    assert report["bz"] < GRAD_RTOL, report
+    # covariance-side gradients: same bound at the 99th percentile
+    for key in ("cov0", "hcov"):
+        assert report[key][0] < GRAD_RTOL, report
+
+
+@pytest.mark.parametrize("ckpt", [1, 2, 4, 10])
+def test_checkpoint_strides_agree(p2r, torch, ckpt):
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch)
+    base = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=5)
+    other = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=ckpt)
+    for key in ("par0", "cov0", "hpos", "hcov", "dr"):
+        assert np.quantile(grad_err(other[key], base[key]), 0.999) < 1e-5, key
+    assert abs(other["bz"] - base["bz"]) <= 1e-5 * abs(base["bz"])
+
+
+def test_forward_outputs_match_plain_forward(p2r, torch):
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch)
+    got = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
+    out = torch.empty(trk.size, dtype=torch.float32, device="cuda")
+    chi2 = torch.empty(cfg.ntracks, dtype=torch.float32, device="cuda")
+    p2r.forward(cfg, d(trk), d(hit), out, chi2=chi2, dr=d(dr))
+    parity.assert_same_arithmetic(got["trk_out"], out.cpu().numpy(), 32, "fwd+bwd forward outputs")
+    c = chi2.cpu().numpy()
+    assert np.quantile(np.abs(got["chi2"] - c) / np.maximum(np.abs(c), 1.0), 0.999) < 1e-5
+
+
+def test_per_event_gradients_sum_to_totals(p2r, torch):
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch, nevts=3, nb=4)
+    got = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, per_event=True)
+    assert np.allclose(got["dr_event"].sum(0), got["dr"], rtol=1e-12, atol=0)
+    assert np.isclose(got["bz_event"].sum(), got["bz"], rtol=1e-12, atol=0)
+    ref = torch_reference(p2r, cfg, trk, hit, dr, g_trk, g_chi2)
+    assert grad_err(got["dr"], ref["dr"]).max() < GRAD_RTOL
+
+
+def test_masked_lanes_adjoint(p2r, torch):
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch, nlayer=25)
+    nlay = np.random.default_rng(9).integers(10, 26, cfg.ntracks).astype(np.int32)
+    ref = torch_reference(p2r, cfg, trk, hit, dr, g_trk, g_chi2, nlay=nlay)
+    got = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, nlay=nlay)
+    for key in ("par0", "hpos", "dr"):
+        assert np.quantile(grad_err(got[key], ref[key]), 0.99) < GRAD_RTOL, key
+    # hits past a track's last layer get zero gradient
+    for t in range(0, cfg.ntracks, 37):
+        assert np.all(got["hpos"][t, nlay[t]:] == 0)
+
+
+def test_autograd_function(p2r, torch):
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
+    t, h, r = d(trk).requires_grad_(), d(hit).requires_grad_(), d(dr).requires_grad_()
+    bz = torch.tensor(3.8, dtype=torch.float64, requires_grad=True)
+    out, chi2 = p2r.P2RChain.apply(t, h, r, bz, cfg, 5)
+    L = (out * d(g_trk)).sum() + (chi2 * d(g_chi2)).sum()
+    L.backward()
+    got = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2)
+    gt = t.grad.cpu().numpy().reshape(cfg.nblocks, 28, 32)
+    assert np.allclose(gt[:, 0:6, :].transpose(0, 2, 1).reshape(-1, 6), got["par0"], rtol=1e-6, atol=0)
+    assert np.allclose(r.grad.cpu().numpy(), got["dr"].astype(np.float32), rtol=1e-6)
+    assert abs(float(bz.grad) - got["bz"]) <= 1e-9 * abs(got["bz"])
+
+
+def test_adjoint_rejects_bad_requests(p2r, torch):
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
+    with pytest.raises(p2r.P2RError):
+        p2r.forward_backward(cfg, d(trk), d(hit), ckpt_stride=3)
+    cfg.mode = p2r.MODE_RESTART
+    with pytest.raises(p2r.P2RError):
+        p2r.forward_backward(cfg, d(trk), d(hit))
