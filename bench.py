@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=10)
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--uneven-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--ref-budget", type=float, default=90.0, help="reference arm: total seconds")
     return ap.parse_args()
@@ -336,6 +339,58 @@ def main():
                                  "parameters/covariance, hits, per-layer dr and Bz of sum(g.out) + sum(chi2)) "
                                  "divided by the plain p2r_forward time")
 
+    # bsize sweep of the fused forward (same tracks re-laid out; autotuned launch shape)
+    sweep = None
+    if not args.no_sweep and world == 1:
+        from p2r_tests_b200 import autotune
+        r = autotune.tune_forward(cfg, trk, hit, bsizes=(32, 64, 128), threads=(64, 96, 128), stages=(2, 4),
+                                  reps=20, use_cache=False)
+        sweep = {}
+        for t in r["tried"]:
+            k = str(t["bsize"])
+            ups = updates / (t["ms"] / 1e3)
+            if k not in sweep or ups > sweep[k]["updates_per_s"]:
+                sweep[k] = {"updates_per_s": ups, "ms": t["ms"], "block_threads": t["block_threads"],
+                            "stages": t["stages"]}
+
+    # uneven batch: 1000 events, log-normal track counts, 10-25 layers per track, one
+    # persistent queue launch captured in a CUDA graph, launch shape picked by the autotuner
+    uneven = None
+    if not args.no_uneven and world == 1:
+        from p2r_tests_b200 import autotune
+        counts = p2r.lognormal_counts(1000, median=2000, sigma=1.0, lo=50, hi=20000, seed=7)
+        wl = {bs: p2r.uneven_workload(counts, bsize=bs, nlayer_max=25) for bs in (32, 64)}
+        tq = autotune.tune_queue(counts, bsizes=(32, 64), granularity=(1, 4, 16), threads=(64, 128),
+                                 stages=(4,), reps=3, use_cache=False, workloads=wl)
+        w = wl[tq["bsize"]]
+        q = p2r.Queue(w, blocks_per_item=tq["blocks_per_item"], block_threads=tq["block_threads"],
+                      stages=tq["stages"])
+        qt = torch.from_numpy(w["trk"].reshape(-1)).to(dev)
+        qh = torch.from_numpy(w["hit"].reshape(-1)).to(dev)
+        qo = torch.empty_like(qt)
+        q.capture(qt, qh, qo)
+        for _ in range(3):
+            q.replay(stream)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(args.uneven_steps):
+            q.replay(stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        gms = g0.elapsed_time(g1) / args.uneven_steps
+        lat = q.event_latency_ns() / 1e6
+        q.release()
+        uneven = {"workload": "1000 events, tracks/event log-normal (median 2000, sigma 1.0) clipped to "
+                              "[50, 20000], layers/track uniform 10..25, chained",
+                  "tracks": int(counts.sum()), "updates": w["updates"], "bsize": tq["bsize"],
+                  "blocks_per_item": tq["blocks_per_item"], "block_threads": tq["block_threads"],
+                  "stages": tq["stages"], "ms_per_step": gms, "updates_per_s": w["updates"] / (gms / 1e3),
+                  "p50_event_ms": float(np.percentile(lat, 50)), "p99_event_ms": float(np.percentile(lat, 99)),
+                  "launch": "CUDA graph (queue init + one persistent kernel)", "steps": args.uneven_steps,
+                  "autotune_candidates": len(tq["tried"])}
+        del qt, qh, qo, wl
+
     # end to end through the host-buffer C-ABI call: H2D + kernels + D2H every step
     h_trk = torch.from_numpy(trk.reshape(-1)).pin_memory().numpy()
     h_hit = torch.from_numpy(hit.reshape(-1)).pin_memory().numpy()
@@ -391,6 +446,8 @@ def main():
                     "steps": args.e2e_steps, "api": "p2r_forward_host (pinned host buffers, 10 chunks)",
                     "output_matches_device_run": bool(ok)},
             "fwd_adjoint": adjoint,
+            "bsize_sweep": sweep,
+            "uneven_batch": uneven,
             "gpu_launches": args.steps,
             "clocks": clk,
             "nonfinite_tracks": nonfinite,

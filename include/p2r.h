@@ -55,6 +55,7 @@ typedef enum p2r_mode { P2R_MODE_RESTART = 0, P2R_MODE_CHAINED = 1 } p2r_mode;
 /* Option bits for p2r_config.flags. */
 #define P2R_FLAG_FP32_DET 0x1u   /* 2x2 residual-covariance determinant in FP32 (default FP64, TBB:457) */
 #define P2R_FLAG_NO_STAGING 0x2u /* read hits with plain loads instead of cp.async staging */
+#define P2R_FLAG_ADJ_FP32 0x4u   /* p2r_forward_backward in FP32 instead of FP64 (faster, ~1e-2 gradients) */
 
 typedef struct p2r_config {
   int32_t bsize;         /* Matriplex lanes per block (TBB:15-17); >= 1 */
@@ -127,6 +128,60 @@ int p2r_count_nonfinite(const void* trk, int64_t nblocks, int32_t bsize, unsigne
 int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void* host_hits, void* host_trk_out,
                      void* dev_trk_in, void* dev_hits, void* dev_trk_out, int32_t nchunks, void* stream);
 
+/* ---------------------------------------------------------------- uneven batches
+ * Persistent work-queue launch (no counterpart in the reference, which runs a fixed
+ * ntrks x nevts grid and drops ntrks % bsize tracks, TBB:22). Events own contiguous block
+ * ranges [event_block_offset[e], event_block_offset[e+1]) of the MPTRK array; hits are
+ * MPHIT blocks lay + b*nlayer as usual (nlayer = layer slots per block, the largest layer
+ * count). Lane `it` of block b runs nlay_lane[b*bsize + it] layers (0 for padding lanes),
+ * CHAINED. Work items (host-planned by p2r_queue_plan, copied to the device) are claimed
+ * by a persistent grid with one atomic counter; no thread waits on another. */
+typedef struct p2r_queue_item {
+  int32_t event; /* event of the range */
+  int32_t nblk;  /* blocks in the range */
+  int64_t block0; /* first block */
+} p2r_queue_item;
+
+typedef struct p2r_queue {
+  int32_t bsize;                     /* multiple of 32 */
+  int32_t nlayer;                    /* layer slots per block (hit blocks per track block) */
+  int64_t nevts;
+  int64_t nblocks;                   /* total MPTRK blocks */
+  double bz;                         /* field [T]; 0 -> 3.8112 */
+  uint32_t flags;                    /* P2R_FLAG_FP32_DET */
+  int32_t block_threads;             /* threads per CTA, 32..128 (0 = 128) */
+  int32_t stages;                    /* hit-staging depth 2 or 4 (0 = 4) */
+  int32_t ctas_per_sm;               /* resident CTAs per SM to launch (0 = occupancy limit) */
+  const int64_t* event_block_offset; /* device, nevts + 1 */
+  const p2r_queue_item* items;       /* device, n_items */
+  int64_t n_items;
+  const int32_t* nlay_lane;          /* device, nblocks * bsize */
+} p2r_queue;
+
+/* Splits every event's blocks into items of at most blocks_per_item blocks, in event order,
+ * into host_items (capacity entries; NULL to only count). Returns the item count, or the
+ * negated p2r_status on error. */
+int64_t p2r_queue_plan(const int64_t* host_event_block_offset, int64_t nevts, int32_t blocks_per_item,
+                       p2r_queue_item* host_items, int64_t capacity);
+
+/* Device workspace for p2r_run_queue (item counter, per-event slice counters). */
+size_t p2r_queue_workspace_size(const p2r_queue* q);
+
+/* One persistent launch over all items (plus a small initialisation kernel). chi2_out
+ * (nullable) per lane; event_done_ns (nullable, nevts) receives the %globaltimer value at
+ * which each event's last slice finished; start_ns (nullable, 1) the earliest CTA start. */
+int p2r_run_queue(const p2r_queue* q, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
+                  unsigned long long* event_done_ns, unsigned long long* start_ns, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
+/* The same launch sequence captured once into a CUDA graph (all pointers are baked in). */
+typedef struct p2r_graph p2r_graph;
+int p2r_queue_graph_create(const p2r_queue* q, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
+                           unsigned long long* event_done_ns, unsigned long long* start_ns, void* workspace,
+                           size_t workspace_bytes, p2r_graph** out);
+int p2r_graph_launch(p2r_graph* g, void* stream);
+int p2r_graph_destroy(p2r_graph* g);
+
 /* ---------------------------------------------------------------- adjoint
  * Fused forward + hand-written adjoint of the CHAINED layer loop (no counterpart in the
  * reference, which has no derivatives). For the scalar
@@ -144,6 +199,10 @@ int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void*
  * (nullable = 0). dr: radius offsets (nullable = 0); nlay_lane: per-track layer counts as
  * in p2r_forward_masked (nullable). The state is stored every ckpt_stride layers (1, 2, 4,
  * 5 or 10; 0 = 5) and the layers between checkpoints are recomputed. nlayer <= 64.
+ * Arithmetic: FP64 throughout (state, trajectory, reverse), so gradients match FP64 finite
+ * differences; its trk_out / chi2_out are that FP64 forward rounded to float (closer to the
+ * exact result than p2r_forward's FP32 chain). cfg->flags & P2R_FLAG_ADJ_FP32 runs the same
+ * kernel in FP32: several times faster, gradients accurate to ~1e-2 where chi2 enters.
  * workspace: device memory of p2r_forward_backward_workspace_size(cfg) bytes, 256-byte
  * aligned (per-warp partial sums of the shared gradients, reduced in a fixed order in
  * double, so results are deterministic). */
@@ -153,6 +212,21 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
                          const float* grad_chi2, void* grad_trk_in, void* grad_hits, double* grad_dr,
                          double* grad_bz, double* grad_dr_event, double* grad_bz_event, int32_t ckpt_stride,
                          void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------- autotuning
+ * Times p2r_forward on the caller's arrays for every (threads[i], stages[j]) pair
+ * (CUDA events on `stream`, one warm-up launch then `reps` launches each) and reports the
+ * fastest; synchronises the stream. The reference has no tuner (its sizes are macros). */
+typedef struct p2r_tune_result {
+  float best_ms;
+  int32_t block_threads, stages, n_tried;
+  int32_t tried_threads[64], tried_stages[64];
+  float tried_ms[64];
+} p2r_tune_result;
+
+int p2r_autotune_forward(const p2r_config* cfg, const void* trk_in, const void* hits, void* trk_out,
+                         const int32_t* threads, int32_t n_threads, const int32_t* stages, int32_t n_stages,
+                         int32_t reps, p2r_tune_result* out, void* stream);
 
 /* ---------------------------------------------------------------- measurement helper
  * FP32 FMA throughput probe (the denominator of the FP32 compute roofline): blocks x

@@ -233,7 +233,8 @@ void load_hit(const float* blk, int bs, int it, Hit<T>& h) {
 
 // Runs every track of `nblocks` Matriplex blocks through its layers.
 //   mode 0 = restart (each layer starts again from the input track, TBB:894),
-//   mode 1 = chained (the state is carried from layer to layer).
+//   mode 1 = chained (the state is carried from layer to layer),
+//   mode 2 = chained propagation only (no KalmanUpdate; for propagateToR-alone checks).
 //   nlay_lane (nullable): per-track layer count; lanes stop updating after it.
 // Output: float path -> MPTRK layout into out_f (28*bsize words per block);
 //         both paths -> per-track par (6) and cov (21) in double into par_d / cov_d
@@ -253,6 +254,8 @@ void run_tracks(const float* trk, const float* hit, long nblocks, int bs, int nl
       st = in;
       T chi2 = 0;
       const int nl = nlay_lane ? nlay_lane[b * bs + it] : nlayer;
+      if (prior_d)  // a lane with no layer keeps its input covariance
+        for (int i = 0; i < 21; ++i) prior_d[(b * bs + it) * 21 + i] = double(st.cov[i]);
       for (int l = 0; l < nlayer && l < nl; ++l) {
         Hit<T> h;
         load_hit(hit + (b * nlayer + l) * hw, bs, it, h);
@@ -261,6 +264,11 @@ void run_tracks(const float* trk, const float* hit, long nblocks, int bs, int nl
           propagate_to_r(in, h.pos, drl, kfact, st);
         else
           propagate_to_r(st, h.pos, drl, kfact, st);
+        if (mode == 2) {  // propagation only: no update, the output covariance is its own scale
+          if (prior_d)
+            for (int i = 0; i < 21; ++i) prior_d[(b * bs + it) * 21 + i] = double(st.cov[i]);
+          continue;
+        }
         if (prior_d)  // covariance entering the last update (the scale its rounding acts on)
           for (int i = 0; i < 21; ++i) prior_d[(b * bs + it) * 21 + i] = double(st.cov[i]);
         // restart: only the last layer's update survives, and so does only its chi2

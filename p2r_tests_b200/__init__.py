@@ -4,17 +4,19 @@ The package `p2r-tests_b200` is spelled `p2r_tests_b200` because Python module n
 cannot contain '-'. The compute path is libp2r_b200.so (hand-written CUDA behind the C ABI
 in include/p2r.h); this package is the Python host side over that ABI.
 """
-from ._lib import (FLAG_FP32_DET, FLAG_NO_STAGING, MODE_CHAINED, MODE_RESTART, P2RError, LIB_PATH, lib)
+from ._lib import (FLAG_ADJ_FP32, FLAG_FP32_DET, FLAG_NO_STAGING, MODE_CHAINED, MODE_RESTART, P2RError, LIB_PATH, lib)
 from .api import (Config, KalmanUpdate, REF_BZ, count_nonfinite, forward, forward_host, fp32_fma_probe, gen_params,
                   generate_fixture,
                   generate_helix, kfact, propagateToR, run_layers, summary, tracks_cov, tracks_par, tracks_q)
 
 from .autograd import P2RChain, forward_backward, workspace_size
+from .uneven import Queue, lognormal_counts, plan, uneven_workload
+from . import autotune
 
 __all__ = [
-    "P2RChain", "forward_backward", "workspace_size",
+    "P2RChain", "forward_backward", "workspace_size", "Queue", "lognormal_counts", "plan", "uneven_workload",
     "Config", "KalmanUpdate", "propagateToR", "run_layers", "forward", "forward_host", "fp32_fma_probe",
     "count_nonfinite", "kfact",
     "gen_params", "generate_helix", "generate_fixture", "summary", "tracks_par", "tracks_cov", "tracks_q",
-    "MODE_CHAINED", "MODE_RESTART", "FLAG_FP32_DET", "FLAG_NO_STAGING", "P2RError", "REF_BZ", "LIB_PATH", "lib",
+    "MODE_CHAINED", "MODE_RESTART", "FLAG_ADJ_FP32", "FLAG_FP32_DET", "FLAG_NO_STAGING", "P2RError", "REF_BZ", "LIB_PATH", "lib",
 ]

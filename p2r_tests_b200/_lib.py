@@ -24,6 +24,7 @@ MODE_RESTART = 0
 MODE_CHAINED = 1
 FLAG_FP32_DET = 0x1
 FLAG_NO_STAGING = 0x2
+FLAG_ADJ_FP32 = 0x4
 
 
 class P2RError(RuntimeError):
@@ -64,6 +65,26 @@ class CGenParams(ctypes.Structure):
     ]
 
 
+class CQueueItem(ctypes.Structure):
+    _fields_ = [("event", ctypes.c_int32), ("nblk", ctypes.c_int32), ("block0", ctypes.c_int64)]
+
+
+class CQueue(ctypes.Structure):
+    _fields_ = [
+        ("bsize", ctypes.c_int32), ("nlayer", ctypes.c_int32), ("nevts", ctypes.c_int64),
+        ("nblocks", ctypes.c_int64), ("bz", ctypes.c_double), ("flags", ctypes.c_uint32),
+        ("block_threads", ctypes.c_int32), ("stages", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32),
+        ("event_block_offset", ctypes.c_void_p), ("items", ctypes.c_void_p), ("n_items", ctypes.c_int64),
+        ("nlay_lane", ctypes.c_void_p),
+    ]
+
+
+class CTuneResult(ctypes.Structure):
+    _fields_ = [("best_ms", ctypes.c_float), ("block_threads", ctypes.c_int32), ("stages", ctypes.c_int32),
+                ("n_tried", ctypes.c_int32), ("tried_threads", ctypes.c_int32 * 64),
+                ("tried_stages", ctypes.c_int32 * 64), ("tried_ms", ctypes.c_float * 64)]
+
+
 class CSummary(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "avg_x", "avg_y", "avg_z", "avg_r", "avg_pt", "avg_phi", "avg_theta",
@@ -90,6 +111,13 @@ SIGNATURES = {
     "p2r_forward_host": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "p2r_fp32_fma_probe": (ctypes.c_int, [_i64, _i32, _i32, _vp, _vp]),
     "p2r_forward_backward_workspace_size": (ctypes.c_size_t, [_cfgp]),
+    "p2r_queue_plan": (ctypes.c_int64, [_vp, _i64, _i32, _vp, _i64]),
+    "p2r_autotune_forward": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _i32, _vp, _i32, _i32, _vp, _vp]),
+    "p2r_queue_workspace_size": (ctypes.c_size_t, [_vp]),
+    "p2r_run_queue": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "p2r_queue_graph_create": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
+    "p2r_graph_launch": (ctypes.c_int, [_vp, _vp]),
+    "p2r_graph_destroy": (ctypes.c_int, [_vp]),
     "p2r_forward_backward": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                             _vp, _vp, _i32, _vp, ctypes.c_size_t, _vp]),
     "p2r_gen_params_default": (None, [ctypes.POINTER(CGenParams)]),

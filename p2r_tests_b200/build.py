@@ -43,10 +43,15 @@ def headers() -> list[Path]:
     return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "p2r.h"])
 
 
+def extra_defines() -> list[str]:
+    """Extra -D options for the CUDA sources, from P2R_DEFINES (e.g. "P2R_FAST_MATH")."""
+    return ["-D" + d for d in os.environ.get("P2R_DEFINES", "").split() if d]
+
+
 def _compile(src: Path, verbose_ptxas: bool) -> tuple[Path, str]:
     obj = BUILD / (src.name + ".o")
     if src.suffix == ".cu":
-        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *extra_defines(), "-c", str(src), "-o", str(obj)]
         if verbose_ptxas:
             cmd += ["-Xptxas", "-v"]
     else:

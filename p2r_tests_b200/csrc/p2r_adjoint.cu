@@ -1,14 +1,22 @@
 // Fused forward + adjoint of the chained layer loop (sm_100a), and its C-ABI entry points.
 //
-// One thread per track. The forward pass is the production chained forward
-// (p2r_math.cuh); it stores the track state every CK layers (thread-local checkpoints).
-// The reverse sweep walks the segments backwards: it recomputes the states inside a
-// segment from its checkpoint, then for each layer, last to first, recomputes that layer
-// with the tape of p2r_adjoint.cuh and runs the hand-written reverse of the update and
-// of the propagation. Gradients produced:
+// One thread per track. The forward pass stores the track state every CK layers
+// (thread-local checkpoints). The reverse sweep walks the segments backwards: it recomputes
+// the states inside a segment from its checkpoint, then for each layer, last to first,
+// recomputes that layer with the tape of p2r_adjoint.cuh and runs the hand-written reverse
+// of the update and of the propagation. Gradients produced:
 //   per track  d/d(initial par, cov), d/d(hit pos, hit cov) for every layer
 //   shared     d/d(dr[layer]) and d/d(Bz), summed over tracks, and optionally per event
 // of L = sum_tracks (g_par . par_final + g_cov . cov_final + g_chi2 * chi2_total).
+//
+// Precision: by default the whole kernel (carried state, trajectory, tape and reverse)
+// runs in FP64. Measured on the synthetic-helix workload: the FP32 chain leaves 0.7 % (p99)
+// of rounding in chi2 (an FP32 position at 100 cm carries ~8e-6 cm, ~1 % of a 10 um
+// residual) and 16-46 % (p99) in d/d(initial parameters) (the filtered state depends on
+// the seed through small differences of large terms); FP64 arithmetic with the state
+// rounded to FP32 between layers still leaves 2e-3 on d chi2/d dr. P2R_FLAG_ADJ_FP32 selects
+// the FP32 kernel (the same code instantiated in float) where that accuracy suffices.
+//
 // Shared sums: each warp reduces with shuffles (fixed order) into per-warp partials in
 // the workspace; a second kernel adds the partials in a fixed order in double, so the
 // results are deterministic run to run.
@@ -17,7 +25,6 @@
 
 #include "p2r_adjoint.cuh"
 #include "p2r_internal.h"
-#include "p2r_math.cuh"
 
 namespace p2r {
 
@@ -40,16 +47,26 @@ struct AdjParams {
   int bsize;
   int nlayer;
   float kfact;
-  float bz;
+  double bz;
 };
 
-__device__ __forceinline__ float warp_sum(float v) {
+template <class T>
+__device__ __forceinline__ T warp_sum_t(T v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
-template <int CK>
+template <class T>
+__device__ __forceinline__ void load_hit_t(const float* h, int bs, int it, T (&hp)[3], T (&hc)[6]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) hp[i] = (T)h[i * bs + it];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) hc[i] = (T)h[(3 + i) * bs + it];
+}
+
+// T: arithmetic type of the whole kernel (float or double). CK: checkpoint stride.
+template <class T, int CK>
 __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
   constexpr int NCK = (kMaxAdjLayers + CK - 1) / CK;
   const int bs = p.bsize;
@@ -61,28 +78,30 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
   const long long gwarp = g >> 5;
   float* wpart = p.partials + gwarp * (p.nlayer + 1);
 
-  float par[6] = {0, 0, 0, 1, 0, 1}, cov[21] = {};
+  T par[6] = {0, 0, 0, 1, 0, 1}, cov[21] = {};
   int q = 1;
   int nl = 0;
   const float* tb = p.trk_in + b * (long long)(28 * bs);
   if (valid) {
 #pragma unroll
-    for (int i = 0; i < 6; ++i) par[i] = tb[i * bs + it];
+    for (int i = 0; i < 6; ++i) par[i] = (T)tb[i * bs + it];
 #pragma unroll
-    for (int i = 0; i < 21; ++i) cov[i] = tb[(6 + i) * bs + it];
+    for (int i = 0; i < 21; ++i) cov[i] = (T)tb[(6 + i) * bs + it];
     q = __float_as_int(tb[27 * bs + it]);
     nl = p.nlay ? min(p.nlayer, max(0, p.nlay[b * bs + it])) : p.nlayer;
   }
-  const float k = (float)q * p.kfact;
-  const float kinv = 1.f / k;
+  // k = q * kfact(Bz) in the kernel's precision (kfact evaluated in double, TBB:654)
+  const T kfact = (sizeof(T) == sizeof(float)) ? (T)p.kfact : (T)(100.0 / (-0.299792458 * p.bz));
+  const T k = (T)q * kfact;
+  const T kinv = T(1) / k;
   int nl_warp = nl;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) nl_warp = max(nl_warp, __shfl_xor_sync(0xffffffffu, nl_warp, o));
   const float* hblk = p.hits + b * (long long)p.nlayer * (9 * bs);
 
   // ---- forward pass with checkpoints every CK layers
-  float ck[NCK][27];
-  float chi2 = 0.f;
+  T ck[NCK][27];
+  T chi2 = 0;
   for (int l = 0; l < nl; ++l) {
     if (l % CK == 0) {
 #pragma unroll
@@ -90,105 +109,86 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
 #pragma unroll
       for (int i = 0; i < 21; ++i) ck[l / CK][6 + i] = cov[i];
     }
-    const float* h = hblk + (long long)l * (9 * bs);
-    float hp[3], hc[6];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) hp[i] = h[i * bs + it];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) hc[i] = h[(3 + i) * bs + it];
-    const float rh = hipo(hp[0], hp[1]);
-    const float rt = p.dr ? rh + p.dr[l] : rh;
-    propagate_to_r(par, cov, k, kinv, rt, par, cov);
-    chi2 += kalman_update<true, true>(par, cov, hp, hc, rh);
+    T hp[3], hc[6];
+    load_hit_t(hblk + (long long)l * (9 * bs), bs, it, hp, hc);
+    chi2 += adj::layer_fwd(par, cov, k, kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0));
   }
   if (valid) {
     if (p.trk_out) {
       float* ob = p.trk_out + b * (long long)(28 * bs);
 #pragma unroll
-      for (int i = 0; i < 6; ++i) ob[i * bs + it] = par[i];
+      for (int i = 0; i < 6; ++i) ob[i * bs + it] = (float)par[i];
 #pragma unroll
-      for (int i = 0; i < 21; ++i) ob[(6 + i) * bs + it] = cov[i];
+      for (int i = 0; i < 21; ++i) ob[(6 + i) * bs + it] = (float)cov[i];
       ob[27 * bs + it] = __int_as_float(q);
     }
-    if (p.chi2_out) p.chi2_out[b * bs + it] = chi2;
+    if (p.chi2_out) p.chi2_out[b * bs + it] = (float)chi2;
   }
 
   // ---- reverse sweep
-  float pb[6] = {}, cb[21] = {};
-  float chi2b = 0.f;
+  T pb[6] = {}, cb[21] = {};
+  T chi2b = 0;
   if (valid) {
     if (p.g_trk_out) {
       const float* gb = p.g_trk_out + b * (long long)(28 * bs);
 #pragma unroll
-      for (int i = 0; i < 6; ++i) pb[i] = gb[i * bs + it];
+      for (int i = 0; i < 6; ++i) pb[i] = (T)gb[i * bs + it];
 #pragma unroll
-      for (int i = 0; i < 21; ++i) cb[i] = gb[(6 + i) * bs + it];
+      for (int i = 0; i < 21; ++i) cb[i] = (T)gb[(6 + i) * bs + it];
     }
-    if (p.g_chi2) chi2b = p.g_chi2[b * bs + it];
+    if (p.g_chi2) chi2b = (T)p.g_chi2[b * bs + it];
   }
-  float kbar = 0.f, kinvbar = 0.f;
+  T kbar = 0, kinvbar = 0;
   const int nseg = (nl_warp + CK - 1) / CK;
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int a = seg * CK;
     const int e = min(a + CK, nl_warp);
     // states before layers a .. e-1 of this segment, recomputed from the checkpoint
-    float st[CK][27];
+    T st[CK][27];
     if (a < nl) {
 #pragma unroll
       for (int i = 0; i < 27; ++i) st[0][i] = ck[seg][i];
     }
     for (int l = a + 1; l < e && l < nl; ++l) {
-      float sp[6], sc[21];
+      T sp[6], sc[21];
 #pragma unroll
       for (int i = 0; i < 6; ++i) sp[i] = st[l - 1 - a][i];
 #pragma unroll
       for (int i = 0; i < 21; ++i) sc[i] = st[l - 1 - a][6 + i];
-      const float* h = hblk + (long long)(l - 1) * (9 * bs);
-      float hp[3], hc[6];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) hp[i] = h[i * bs + it];
-#pragma unroll
-      for (int i = 0; i < 6; ++i) hc[i] = h[(3 + i) * bs + it];
-      const float rh = hipo(hp[0], hp[1]);
-      const float rt = p.dr ? rh + p.dr[l - 1] : rh;
-      propagate_to_r(sp, sc, k, kinv, rt, sp, sc);
-      kalman_update<true, false>(sp, sc, hp, hc, rh);
+      T hp[3], hc[6];
+      load_hit_t(hblk + (long long)(l - 1) * (9 * bs), bs, it, hp, hc);
+      adj::layer_fwd(sp, sc, k, kinv, hp, hc, p.dr ? (T)p.dr[l - 1] : T(0));
 #pragma unroll
       for (int i = 0; i < 6; ++i) st[l - a][i] = sp[i];
 #pragma unroll
       for (int i = 0; i < 21; ++i) st[l - a][6 + i] = sc[i];
     }
     for (int l = e - 1; l >= a; --l) {
-      float drb = 0.f;
+      T drb = 0;
       if (l < nl) {
-        float sp[6], sc[21];
+        T sp[6], sc[21];
 #pragma unroll
         for (int i = 0; i < 6; ++i) sp[i] = st[l - a][i];
 #pragma unroll
         for (int i = 0; i < 21; ++i) sc[i] = st[l - a][6 + i];
-        const float* h = hblk + (long long)l * (9 * bs);
-        float hp[3], hc[6];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) hp[i] = h[i * bs + it];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) hc[i] = h[(3 + i) * bs + it];
-        const float drl = p.dr ? p.dr[l] : 0.f;
-        float hpb[3], hcb[6];
-        adj::layer_rev(sp, sc, k, kinv, hp, hc, drl, pb, cb, chi2b, hpb, hcb, drb, kbar, kinvbar);
+        T hp[3], hc[6], hpb[3], hcb[6];
+        load_hit_t(hblk + (long long)l * (9 * bs), bs, it, hp, hc);
+        adj::layer_rev(sp, sc, k, kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0), pb, cb, chi2b, hpb, hcb, drb, kbar,
+                       kinvbar);
         if (p.g_hits) {
           float* gh = p.g_hits + (b * (long long)p.nlayer + l) * (9 * bs);
 #pragma unroll
-          for (int i = 0; i < 3; ++i) gh[i * bs + it] = hpb[i];
+          for (int i = 0; i < 3; ++i) gh[i * bs + it] = (float)hpb[i];
 #pragma unroll
-          for (int i = 0; i < 6; ++i) gh[(3 + i) * bs + it] = hcb[i];
+          for (int i = 0; i < 6; ++i) gh[(3 + i) * bs + it] = (float)hcb[i];
         }
       } else if (valid && p.g_hits) {
         float* gh = p.g_hits + (b * (long long)p.nlayer + l) * (9 * bs);
 #pragma unroll
         for (int i = 0; i < 9; ++i) gh[i * bs + it] = 0.f;
       }
-      drb = warp_sum(drb);
-      if (lane == 0) wpart[l] = drb;
+      drb = warp_sum_t(drb);
+      if (lane == 0) wpart[l] = (float)drb;
     }
   }
   // layers the whole warp skipped have zero gradient
@@ -201,15 +201,15 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
       for (int i = 0; i < 9; ++i) gh[i * bs + it] = 0.f;
     }
   // k = q * kfact(Bz): dk/dBz = -k / Bz
-  float bzb = valid ? (kbar - kinvbar * kinv * kinv) * (-k / p.bz) : 0.f;
-  bzb = warp_sum(bzb);
-  if (lane == 0) wpart[p.nlayer] = bzb;
+  T bzb = valid ? (kbar - kinvbar * kinv * kinv) * (-k / (T)p.bz) : T(0);
+  bzb = warp_sum_t(bzb);
+  if (lane == 0) wpart[p.nlayer] = (float)bzb;
   if (valid && p.g_trk_in) {
     float* gb = p.g_trk_in + b * (long long)(28 * bs);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) gb[i * bs + it] = pb[i];
+    for (int i = 0; i < 6; ++i) gb[i * bs + it] = (float)pb[i];
 #pragma unroll
-    for (int i = 0; i < 21; ++i) gb[(6 + i) * bs + it] = cb[i];
+    for (int i = 0; i < 21; ++i) gb[(6 + i) * bs + it] = (float)cb[i];
     gb[27 * bs + it] = 0.f;
   }
 }
@@ -279,11 +279,22 @@ WsLayout layout_of(const p2r_config* cfg) {
   return w;
 }
 
-template <int CK>
+template <class T, int CK>
 cudaError_t launch_fwdbwd(const AdjParams& p, long long ntr, cudaStream_t st) {
   const long long grid = (ntr + kAdjThreads - 1) / kAdjThreads;
-  fwdbwd_kernel<CK><<<(unsigned)grid, kAdjThreads, 0, st>>>(p);
+  fwdbwd_kernel<T, CK><<<(unsigned)grid, kAdjThreads, 0, st>>>(p);
   return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_fwdbwd_ck(const AdjParams& p, long long ntr, int ck, cudaStream_t st) {
+  switch (ck) {
+    case 1: return launch_fwdbwd<T, 1>(p, ntr, st);
+    case 2: return launch_fwdbwd<T, 2>(p, ntr, st);
+    case 4: return launch_fwdbwd<T, 4>(p, ntr, st);
+    case 10: return launch_fwdbwd<T, 10>(p, ntr, st);
+    default: return launch_fwdbwd<T, 5>(p, ntr, st);
+  }
 }
 
 }  // namespace
@@ -331,20 +342,17 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   p.bsize = cfg->bsize;
   p.nlayer = cfg->nlayer;
   p.kfact = p2r_kfact_of(cfg->bz);
-  p.bz = (float)(cfg->bz == 0.0 ? 3.8112 : cfg->bz);
+  p.bz = cfg->bz == 0.0 ? 3.8112 : cfg->bz;
   const long long ntr = nblocks * cfg->bsize;
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
-  switch (ckpt_stride) {
-    case 1: e = launch_fwdbwd<1>(p, ntr, st); break;
-    case 2: e = launch_fwdbwd<2>(p, ntr, st); break;
-    case 4: e = launch_fwdbwd<4>(p, ntr, st); break;
-    case 0:
-    case 5: e = launch_fwdbwd<5>(p, ntr, st); break;
-    case 10: e = launch_fwdbwd<10>(p, ntr, st); break;
-    default:
-      return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: checkpoint stride %d (use 1, 2, 4, 5 or 10)", who, ckpt_stride);
-  }
+  if (ckpt_stride != 0 && ckpt_stride != 1 && ckpt_stride != 2 && ckpt_stride != 4 && ckpt_stride != 5 &&
+      ckpt_stride != 10)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: checkpoint stride %d (use 1, 2, 4, 5 or 10)", who, ckpt_stride);
+  if (cfg->flags & P2R_FLAG_ADJ_FP32)
+    e = launch_fwdbwd_ck<float>(p, ntr, ckpt_stride, st);
+  else
+    e = launch_fwdbwd_ck<double>(p, ntr, ckpt_stride, st);
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: launch failed: %s", who, cudaGetErrorString(e));
   const int nout = cfg->nlayer + 1;
   double* ev = (double*)((char*)workspace + w.event_off);

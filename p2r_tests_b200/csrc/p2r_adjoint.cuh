@@ -21,6 +21,11 @@
 #else
 #define P2R_HD inline
 #endif
+#if defined(__CUDA_ARCH__)
+#define P2R_UNROLL _Pragma("unroll")
+#else
+#define P2R_UNROLL
+#endif
 
 namespace p2r {
 namespace adj {
@@ -89,7 +94,7 @@ P2R_HD void prop_fwd(const T (&ip)[6], const T (&ic)[21], T k, T kinv, T r, Prop
   T dDdipt = 0, dDdphi = 0, D = 0, sina, cosa, omc;
   T xo = xin, yo = yin;
   const T pt = t.pt;
-#pragma unroll
+P2R_UNROLL
   for (int i = 0; i < 5; ++i) {
     t.xo[i] = xo;
     t.yo[i] = yo;
@@ -154,7 +159,7 @@ P2R_HD void prop_fwd(const T (&ip)[6], const T (&ic)[21], T k, T kinv, T r, Prop
   t.J41 = dady;
   t.J43 = dadipt;
   t.J44 = T(1) + dadphi;
-#pragma unroll
+P2R_UNROLL
   for (int j = 0; j < 6; ++j) {
     const T c0 = ic[S6(0, j)], c1 = ic[S6(1, j)], c2 = ic[S6(2, j)], c3 = ic[S6(3, j)], c4 = ic[S6(4, j)],
             c5 = ic[S6(5, j)];
@@ -164,10 +169,10 @@ P2R_HD void prop_fwd(const T (&ip)[6], const T (&ic)[21], T k, T kinv, T r, Prop
     t.T4[j] = t.J40 * c0 + t.J41 * c1 + t.J43 * c3 + t.J44 * c4;
   }
   // C' = (J C) J^T, lower triangle; rows 3 and 5 of J C are rows 3 and 5 of C
-#pragma unroll
+P2R_UNROLL
   for (int i = 0; i < 6; ++i) {
     T Ti[6];
-#pragma unroll
+P2R_UNROLL
     for (int j = 0; j < 6; ++j)
       Ti[j] = i == 0 ? t.T0[j] : i == 1 ? t.T1[j] : i == 2 ? t.T2[j] : i == 4 ? t.T4[j] : ic[S6(i, j)];
     oc[S6(i, 0)] = Ti[0] * t.J00 + Ti[1] * t.J01 + Ti[3] * t.J03 + Ti[4] * t.J04;
@@ -209,12 +214,12 @@ P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], 
 
   // ---- C' = J C J^T: S = Gbar + Gbar^T, Jbar = S (J C), cbar = packed(J^T S J)
   T S[6][6];
-#pragma unroll
+P2R_UNROLL
   for (int i = 0; i < 6; ++i)
-#pragma unroll
+P2R_UNROLL
     for (int j = 0; j < 6; ++j) S[i][j] = i == j ? T(2) * cb_out[S6(i, i)] : cb_out[S6(i, j)];
   T Tf[6][6];
-#pragma unroll
+P2R_UNROLL
   for (int j = 0; j < 6; ++j) {
     Tf[0][j] = t.T0[j];
     Tf[1][j] = t.T1[j];
@@ -225,7 +230,7 @@ P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], 
   }
   auto ST = [&](int a, int b) {
     T s = 0;
-#pragma unroll
+P2R_UNROLL
     for (int c = 0; c < 6; ++c) s += S[a][c] * Tf[c][b];
     return s;
   };
@@ -235,7 +240,7 @@ P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], 
   const T J40b = ST(4, 0), J41b = ST(4, 1), J43b = ST(4, 3), J44b = ST(4, 4);
   // W = S J, M = J^T W
   T W[6][6];
-#pragma unroll
+P2R_UNROLL
   for (int a = 0; a < 6; ++a) {
     W[a][0] = S[a][0] * t.J00 + S[a][1] * t.J10 + S[a][2] * t.J20 + S[a][4] * t.J40;
     W[a][1] = S[a][0] * t.J01 + S[a][1] * t.J11 + S[a][2] * t.J21 + S[a][4] * t.J41;
@@ -244,7 +249,7 @@ P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], 
     W[a][4] = S[a][0] * t.J04 + S[a][1] * t.J14 + S[a][2] * t.J24 + S[a][4] * t.J44;
     W[a][5] = S[a][2] * t.J25 + S[a][5];
   }
-#pragma unroll
+P2R_UNROLL
   for (int j = 0; j < 6; ++j) {
     T M[6];
     M[0] = t.J00 * W[0][j] + t.J10 * W[1][j] + t.J20 * W[2][j] + t.J40 * W[4][j];
@@ -253,7 +258,7 @@ P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], 
     M[3] = t.J03 * W[0][j] + t.J13 * W[1][j] + t.J23 * W[2][j] + W[3][j] + t.J43 * W[4][j];
     M[4] = t.J04 * W[0][j] + t.J14 * W[1][j] + t.J24 * W[2][j] + t.J44 * W[4][j];
     M[5] = t.J25 * W[2][j] + W[5][j];
-#pragma unroll
+P2R_UNROLL
     for (int i = j; i < 6; ++i) cb_in[S6(i, j)] = i == j ? T(0.5f) * M[i] : M[i];
   }
 
@@ -352,7 +357,7 @@ P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], 
 
   // ---- the five helix iterations, last to first
   T pxb = 0, pyb = 0;
-#pragma unroll
+P2R_UNROLL
   for (int i = 4; i >= 0; --i) {
     const T xo = t.xo[i], yo = t.yo[i], px = t.px[i], py = t.py[i], r0 = t.r0[i];
     const T id = r - r0;
@@ -490,7 +495,7 @@ P2R_HD T upd_fwd(T (&p)[6], T (&c)[21], const T (&hp)[3], const T (&hc)[6]) {
   const T s = T(1.0 / det);
   const T i0 = s * e2, i1 = e1 * -s, i2 = s * e0;
   T K0[6], K1[6];
-#pragma unroll
+P2R_UNROLL
   for (int m = 0; m < 6; ++m) {
     const T cm0 = c[S6(m, 0)], cm1 = c[S6(m, 1)], cm2 = c[S6(m, 2)];
     K0[m] = cm0 * (R00 * i0) + cm1 * (R01 * i0) + cm2 * i1;
@@ -499,15 +504,15 @@ P2R_HD T upd_fwd(T (&p)[6], T (&c)[21], const T (&hp)[3], const T (&hc)[6]) {
   const T res0 = R00 * (hp[0] - p[0]) + R01 * (hp[1] - p[1]);
   const T res1 = hp[2] - p[2];
   const T chi2 = i0 * res0 * res0 + T(2) * i1 * res0 * res1 + i2 * res1 * res1;
-#pragma unroll
+P2R_UNROLL
   for (int m = 0; m < 6; ++m) p[m] = p[m] + K0[m] * res0 + K1[m] * res1;
   T nc[21];
-#pragma unroll
+P2R_UNROLL
   for (int i = 0; i < 6; ++i)
-#pragma unroll
+P2R_UNROLL
     for (int j = 0; j <= i; ++j)
       nc[S6(i, j)] = c[S6(i, j)] - (K0[i] * R00 * c[S6(0, j)] + K0[i] * R01 * c[S6(1, j)] + K1[i] * c[S6(2, j)]);
-#pragma unroll
+P2R_UNROLL
   for (int i = 0; i < 21; ++i) c[i] = nc[i];
   return chi2;
 }
@@ -522,14 +527,14 @@ P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T
   const T den = T(2) * rh;
   const T R00 = -(hp[1] + p[1]) / den, R01 = (hp[0] + p[0]) / den;
   T A[6];
-#pragma unroll
+P2R_UNROLL
   for (int k = 0; k < 6; ++k) A[k] = c[k] + hc[k];
   const T e0 = R00 * R00 * A[0] + T(2) * R00 * R01 * A[1] + R01 * R01 * A[2];
   const T e1 = A[3] * R00 + A[4] * R01, e2 = A[5];
   const T s = T(1) / (e0 * e2 - e1 * e1);
   const T i0 = s * e2, i1 = -s * e1, i2 = s * e0;
   T B0[6], B1[6], K0[6], K1[6];
-#pragma unroll
+P2R_UNROLL
   for (int m = 0; m < 6; ++m) {
     B0[m] = R00 * c[S6(m, 0)] + R01 * c[S6(m, 1)];
     B1[m] = c[S6(m, 2)];
@@ -540,15 +545,15 @@ P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T
 
   // C' = C - K0 B0^T - K1 B1^T (lower triangle); p' = p + K0 res0 + K1 res1
   T K0b[6], K1b[6], B0b[6], B1b[6];
-#pragma unroll
+P2R_UNROLL
   for (int m = 0; m < 6; ++m) {
     T a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-#pragma unroll
+P2R_UNROLL
     for (int j = 0; j <= m; ++j) {
       a0 += cb[S6(m, j)] * B0[j];
       a1 += cb[S6(m, j)] * B1[j];
     }
-#pragma unroll
+P2R_UNROLL
     for (int i = m; i < 6; ++i) {
       b0 += cb[S6(i, m)] * K0[i];
       b1 += cb[S6(i, m)] * K1[i];
@@ -559,7 +564,7 @@ P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T
     B1b[m] = -b1;
   }
   T res0b = 0, res1b = 0;
-#pragma unroll
+P2R_UNROLL
   for (int m = 0; m < 6; ++m) {
     res0b += pb[m] * K0[m];
     res1b += pb[m] * K1[m];
@@ -569,7 +574,7 @@ P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T
   res0b += chi2b * (T(2) * i0 * res0 + T(2) * i1 * res1);
   res1b += chi2b * (T(2) * i1 * res0 + T(2) * i2 * res1);
   // K0 = B0 i0 + B1 i1, K1 = B0 i1 + B1 i2
-#pragma unroll
+P2R_UNROLL
   for (int m = 0; m < 6; ++m) {
     i0b += K0b[m] * B0[m];
     i1b += K0b[m] * B1[m] + K1b[m] * B0[m];
@@ -579,7 +584,7 @@ P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T
   }
   // B0_m = R00 C_m0 + R01 C_m1, B1_m = C_m2 (cb keeps the direct C' = C ... path)
   T R00b = 0, R01b = 0;
-#pragma unroll
+P2R_UNROLL
   for (int m = 0; m < 6; ++m) {
     R00b += B0b[m] * c[S6(m, 0)];
     R01b += B0b[m] * c[S6(m, 1)];
@@ -612,7 +617,7 @@ P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T
   hcb[3] = e1b * R00;
   hcb[4] = e1b * R01;
   hcb[5] = e2b;
-#pragma unroll
+P2R_UNROLL
   for (int k = 0; k < 6; ++k) cb[k] += hcb[k];
   // R00 = -(hy + y)/den, R01 = (hx + x)/den, den = 2 hipo(hx, hy)
   hpb[1] -= R00b / den;
@@ -649,9 +654,9 @@ P2R_HD void layer_rev(const T (&p)[6], const T (&c)[21], T k, T kinv, const T (&
   upd_rev(pp, pc, hp, hc, pb, cb, chi2b, hpb, hcb);
   T pin[6], cin[21], rbar = 0;
   prop_rev(t, p, c, k, kinv, r, pb, cb, pin, cin, rbar, kbar, kinvbar);
-#pragma unroll
+P2R_UNROLL
   for (int i = 0; i < 6; ++i) pb[i] = pin[i];
-#pragma unroll
+P2R_UNROLL
   for (int i = 0; i < 21; ++i) cb[i] = cin[i];
   drb += rbar;
   if (rh > T(0)) {

@@ -75,6 +75,56 @@ __device__ __forceinline__ void store_track(float* blk, int bs, int it, const fl
   __stcs(blk + 27 * bs + it, __int_as_float(q));
 }
 
+// One warp's 32-lane slice of one Matriplex block through its layers, chained, with the
+// hits staged per warp through the cp.async ring `ring` (STAGES x 288 floats of shared
+// memory). Lane `lane` owns lane `it` of block `b`; lanes run layers [0, nlay) (MASK: the
+// per-track count, else p.nlayer) and the warp iterates to its largest count. All 32 lanes
+// must call it together (bs % 32 == 0).
+template <int BS, int STAGES, bool CHI2, bool DR, bool MASK, bool FP64DET>
+__device__ __forceinline__ void chained_slice_staged(const FwdParams& p, long long b, int it, int lane, float* ring) {
+  const int bs = BS > 0 ? BS : p.bsize;
+  float par[6], cov[21];
+  int q;
+  load_track(p.trk_in + b * (long long)(kTrkWords * bs), bs, it, par, cov, q);
+  const float k = (float)q * p.kfact;
+  const float kinv = 1.f / k;
+  int nl = p.nlayer;
+  if (MASK) nl = min(nl, max(0, p.nlay[b * bs + it]));
+  const int nl_warp = MASK ? __reduce_max_sync(0xffffffffu, nl) : nl;
+  const float* slice = p.hits + b * (long long)p.nlayer * (kHitWords * bs) + (it - lane);
+  const long long lstride = (long long)kHitWords * bs;
+  float chi2 = 0.f;
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < nl_warp) stage_hit_slice(ring + s * 288, slice + s * lstride, bs, lane);
+    cp_async_commit();
+  }
+  for (int l = 0; l < nl_warp; ++l) {
+    const int ln = l + STAGES - 1;
+    if (ln < nl_warp) stage_hit_slice(ring + (ln % STAGES) * 288, slice + ln * lstride, bs, lane);
+    cp_async_commit();
+    cp_async_wait<STAGES - 1>();
+    __syncwarp();
+    const float* st = ring + (l % STAGES) * 288;
+    float hp[3], hc[6];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) hp[i] = st[i * 32 + lane];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) hc[i] = st[(3 + i) * 32 + lane];
+    __syncwarp();  // the stage may be refilled from the next iteration on
+    if (!MASK || l < nl) {
+      const float rh = hipo(hp[0], hp[1]);
+      const float rt = DR ? rh + __ldg(p.dr + l) : rh;
+      propagate_to_r(par, cov, k, kinv, rt, par, cov);
+      chi2 += kalman_update<FP64DET, CHI2>(par, cov, hp, hc, rh);
+    }
+  }
+  cp_async_wait<0>();
+  __syncwarp();  // no lane reuses the ring before every lane's copies have landed
+  store_track(p.trk_out + b * (long long)(kTrkWords * bs), bs, it, par, cov, q);
+  if (CHI2) p.chi2[b * bs + it] = chi2;
+}
+
 // BS: compile-time bsize (0 = run-time p.bsize). STAGED requires bsize % 32 == 0.
 template <int BS, int STAGES, bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET>
 __global__ void __launch_bounds__(128) fwd_kernel(FwdParams p) {

@@ -19,7 +19,22 @@ namespace p2r {
 // packed lower-triangle index of a symmetric 6x6 (TBB:46-54)
 __host__ __device__ constexpr int S6(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
 
-__device__ __forceinline__ float hipo(float x, float y) { return sqrtf(x * x + y * y); }
+// Division and square root. With P2R_FAST_MATH defined they are the hardware
+// approximations (div.approx / sqrt.approx, about 2 ulp) instead of the IEEE-rounded
+// sequences; every other operation is unchanged.
+#ifdef P2R_FAST_MATH
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float fsqrt(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+#else
+__device__ __forceinline__ float fdiv(float a, float b) { return a / b; }
+__device__ __forceinline__ float fsqrt(float x) { return sqrtf(x); }
+#endif
+
+__device__ __forceinline__ float hipo(float x, float y) { return fsqrt(x * x + y * y); }
 
 // 4th-order cos / 3rd-order sin for the small per-step turning angles (TBB:644-652).
 // omc = 1 - c, evaluated as x^2/2 - x^4/24: the same polynomial without forming 1 - (1 - ...)
@@ -40,15 +55,15 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
   const float xin = ip[0], yin = ip[1], zin = ip[2];
   const float iptin = ip[3], phiin = ip[4], thetain = ip[5];
   float r0 = hipo(xin, yin);
-  const float pt = 1.f / iptin;
+  const float pt = fdiv(1.f, iptin);
 
   float D = 0.f, cosa = 0.f, sina = 0.f, omc = 0.f;
   float sinP, cosP;
   sincosf(phiin, &sinP, &cosP);  // phi can be large: no approximation (TBB:688-689)
   float pxin = cosP * pt;
   float pyin = sinP * pt;
-  float dDdx = r0 > 0.f ? -xin / r0 : 0.f;
-  float dDdy = r0 > 0.f ? -yin / r0 : 0.f;
+  float dDdx = r0 > 0.f ? -fdiv(xin, r0) : 0.f;
+  float dDdy = r0 > 0.f ? -fdiv(yin, r0) : 0.f;
   float dDdipt = 0.f, dDdphi = 0.f;
   float xo = xin, yo = yin;
 
@@ -60,7 +75,7 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
     sincos4(id * iptin * kinv, sina, cosa, omc);
     if (i + 1 != 5) {
       // path derivatives, only once the step is below 1 um (TBB:714)
-      const float oor0 = (r0 > 0.f && fabsf(r - r0) < 0.0001f) ? 1.f / r0 : 0.f;
+      const float oor0 = (r0 > 0.f && fabsf(r - r0) < 0.0001f) ? fdiv(1.f, r0) : 0.f;
       const float dadipt = id * kinv;
       const float dadx = -xo * iptin * kinv * oor0;
       const float dady = -yo * iptin * kinv * oor0;
@@ -103,7 +118,7 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
   const float J14 = k * (sinP * dadphi * cosa + cosP * dadphi * sina + sinP * cosa + cosP * sina - sinP) * pt;
   float sinT, cosT;
   sincosf(thetain, &sinT, &cosT);  // theta can be large: no approximation (TBB:767-769)
-  const float isinT = 1.f / sinT;
+  const float isinT = fdiv(1.f, sinT);
   const float J20 = k * cosT * dadx * pt * isinT;
   const float J21 = k * cosT * dady * pt * isinT;
   const float J23 = k * cosT * (iptin * dadipt - alpha) * pt * pt * isinT;
@@ -164,8 +179,14 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
 template <bool kFp64Det, bool kChi2>
 __device__ __forceinline__ float kalman_update(float (&p)[6], float (&c)[21], const float (&hp)[3],
                                                const float (&hc)[6], float rhit) {
+#ifdef P2R_FAST_MATH
+  const float inv2r = fdiv(0.5f, rhit);
+  const float rotT00 = -(hp[1] + p[1]) * inv2r;
+  const float rotT01 = (hp[0] + p[0]) * inv2r;
+#else
   const float rotT00 = -(hp[1] + p[1]) / (2.f * rhit);
   const float rotT01 = (hp[0] + p[0]) / (2.f * rhit);
+#endif
 
   const float e0 = (rotT00 * (c[0] + hc[0]) + rotT01 * (c[1] + hc[1])) * rotT00 +
                    (rotT00 * (c[1] + hc[1]) + rotT01 * (c[2] + hc[2])) * rotT01;
@@ -173,10 +194,15 @@ __device__ __forceinline__ float kalman_update(float (&p)[6], float (&c)[21], co
   const float e2 = c[5] + hc[5];
   float s;
   if (kFp64Det) {
+    // the cancellation is in the products' difference: take it in FP64 (TBB:457-458)
     const double det = (double)e0 * e2 - (double)e1 * e1;
+#ifdef P2R_FAST_MATH
+    s = fdiv(1.f, (float)det);  // the reciprocal of the rounded difference needs no FP64
+#else
     s = (float)(1.0 / det);
+#endif
   } else {
-    s = 1.f / (e0 * e2 - e1 * e1);
+    s = fdiv(1.f, e0 * e2 - e1 * e1);
   }
   const float i0 = s * e2;
   const float i1 = e1 * -s;

@@ -1,0 +1,285 @@
+// Persistent work-queue launch for uneven batches: events with different track counts
+// (blocks padded to bsize, padding lanes carry zero layers) and tracks with different layer
+// counts run in ONE launch. The reference has no such mode: it runs a fixed ntrks x nevts
+// grid (TBB:870-926) and silently drops ntrks % bsize tracks (nb = ntrks/bsize, TBB:22).
+//
+// Work items are (event, first block, block count) ranges planned on the host. A grid of
+// (SMs x resident CTAs) CTAs pulls items from an atomic counter; each warp of a CTA takes
+// 32-lane slices of the item's blocks and runs them with the chained staged body of the
+// fused forward. When the last slice of an event finishes, its warp records %globaltimer
+// into event_done_ns[event], giving per-event completion times. No thread waits on another
+// (items are claimed with one atomicAdd), so there is no spin loop to bound.
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cmath>
+#include <new>
+
+#include "p2r_fwd.cuh"
+#include "p2r_internal.h"
+
+namespace p2r {
+
+struct QueueParams {
+  FwdParams f;  // arrays, bsize, nlayer (= layer slots per block), kfact; f.nlay per lane
+  const p2r_queue_item* items;
+  long long n_items;
+  int* counter;                 // next item
+  int* ev_remaining;            // slices left per event
+  unsigned long long* ev_done;  // nullable
+  unsigned long long* t_start;  // nullable
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__global__ void queue_init_kernel(const int64_t* ev_off, long long nevts, int slices_per_block, int* counter,
+                                  int* ev_remaining, unsigned long long* t_start) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < nevts) ev_remaining[e] = (int)((ev_off[e + 1] - ev_off[e]) * slices_per_block);
+  if (e == 0) {
+    *counter = 0;
+    if (t_start) *t_start = ULLONG_MAX;
+  }
+}
+
+template <int BS, int STAGES, bool CHI2, bool FP64DET>
+__global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
+  extern __shared__ __align__(16) float smem[];
+  __shared__ int s_item;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int bs = BS > 0 ? BS : q.f.bsize;
+  const int spb = bs / 32;  // 32-lane slices per block
+  float* ring = smem + warp * (STAGES * 288);
+  if (threadIdx.x == 0 && q.t_start) atomicMin(q.t_start, globaltimer_ns());
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(q.counter, 1);
+    __syncthreads();
+    const long long item = s_item;
+    __syncthreads();  // every thread has read s_item before thread 0 claims the next one
+    if (item >= q.n_items) break;
+    const p2r_queue_item qi = q.items[item];
+    const int nslices = qi.nblk * spb;
+    for (int s = warp; s < nslices; s += nwarps) {
+      const long long b = qi.block0 + s / spb;
+      const int it = (s % spb) * 32 + lane;
+      chained_slice_staged<BS, STAGES, CHI2, false, true, FP64DET>(q.f, b, it, lane, ring);
+      if (lane == 0) {
+        __threadfence();
+        if (atomicSub(&q.ev_remaining[qi.event], 1) == 1 && q.ev_done) q.ev_done[qi.event] = globaltimer_ns();
+      }
+    }
+  }
+}
+
+template <int BS, int STAGES, bool CHI2, bool FP64DET>
+cudaError_t launch_queue_t(const QueueParams& q, int threads, int ctas_per_sm, cudaStream_t st) {
+  auto kern = queue_kernel<BS, STAGES, CHI2, FP64DET>;
+  const size_t smem = (size_t)(threads / 32) * STAGES * 288 * sizeof(float);
+  int dev = 0, sms = 0, occ = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+  if (e != cudaSuccess) return e;
+  const int per_sm = ctas_per_sm > 0 ? (ctas_per_sm < occ ? ctas_per_sm : occ) : occ;
+  const long long want = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  const long long grid = want < q.n_items ? want : (q.n_items > 0 ? q.n_items : 1);
+  kern<<<(unsigned)grid, threads, smem, st>>>(q);
+  return cudaGetLastError();
+}
+
+template <int STAGES, bool CHI2, bool FP64DET>
+cudaError_t launch_queue_bs(const QueueParams& q, int threads, int ctas, cudaStream_t st) {
+  switch (q.f.bsize) {
+    case 32: return launch_queue_t<32, STAGES, CHI2, FP64DET>(q, threads, ctas, st);
+    case 64: return launch_queue_t<64, STAGES, CHI2, FP64DET>(q, threads, ctas, st);
+    case 128: return launch_queue_t<128, STAGES, CHI2, FP64DET>(q, threads, ctas, st);
+    default: return launch_queue_t<0, STAGES, CHI2, FP64DET>(q, threads, ctas, st);
+  }
+}
+
+}  // namespace p2r
+
+using namespace p2r;
+
+namespace {
+
+struct QueueWs {
+  size_t counter_off, start_off, remaining_off, bytes;
+};
+
+QueueWs queue_ws(int64_t nevts) {
+  QueueWs w;
+  w.counter_off = 0;
+  w.start_off = 256;
+  w.remaining_off = 512;
+  w.bytes = 512 + (((size_t)nevts * sizeof(int) + 255) & ~(size_t)255);
+  return w;
+}
+
+int check_queue(const p2r_queue* q, const char* who) {
+  if (!q) return p2r_set_errorf(P2R_ERR_INVALID, "%s: queue is null", who);
+  if (q->bsize < 32 || q->bsize % 32 != 0 || q->bsize > 4096)
+    return p2r_set_errorf(P2R_ERR_QUEUE, "%s: bsize %d must be a multiple of 32", who, q->bsize);
+  if (q->nlayer < 1 || q->nlayer > 4096) return p2r_set_errorf(P2R_ERR_QUEUE, "%s: nlayer %d", who, q->nlayer);
+  if (q->nevts < 0 || q->nblocks < 0 || q->n_items < 0 || q->nevts > INT_MAX)
+    return p2r_set_errorf(P2R_ERR_QUEUE, "%s: negative or too large sizes", who);
+  if (q->n_items > INT_MAX - 65536) return p2r_set_errorf(P2R_ERR_QUEUE, "%s: too many work items", who);
+  if (q->nblocks > 0 && (!q->event_block_offset || !q->items || !q->nlay_lane))
+    return p2r_set_errorf(P2R_ERR_QUEUE, "%s: event offsets, items and layer counts are required", who);
+  if (q->block_threads != 0 && (q->block_threads % 32 || q->block_threads > 128))
+    return p2r_set_errorf(P2R_ERR_INVALID, "%s: block_threads must be a multiple of 32 up to 128", who);
+  if (q->stages != 0 && q->stages != 2 && q->stages != 4)
+    return p2r_set_errorf(P2R_ERR_INVALID, "%s: stages must be 2 or 4", who);
+  if (!std::isfinite(q->bz)) return p2r_set_errorf(P2R_ERR_INVALID, "%s: bz is not finite", who);
+  return P2R_OK;
+}
+
+int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
+                  unsigned long long* event_done_ns, unsigned long long* start_ns, void* workspace, size_t ws_bytes,
+                  cudaStream_t st, const char* who) {
+  int rc = check_queue(q, who);
+  if (rc) return rc;
+  const QueueWs w = queue_ws(q->nevts);
+  if (!workspace || ws_bytes < w.bytes)
+    return p2r_set_errorf(P2R_ERR_WORKSPACE, "%s: workspace of %zu bytes needed", who, w.bytes);
+  if (((uintptr_t)workspace & 255u) != 0) return p2r_set_errorf(P2R_ERR_INVALID, "%s: workspace must be 256-byte aligned", who);
+  if (q->nevts == 0 || q->n_items == 0) return p2r_clear_error();
+  if (!trk_in || !hits || !trk_out) return p2r_set_errorf(P2R_ERR_INVALID, "%s: null array pointer", who);
+  if (((uintptr_t)hits & 15u) != 0) return p2r_set_errorf(P2R_ERR_INVALID, "%s: hits must be 16-byte aligned", who);
+  QueueParams qp;
+  qp.f.trk_in = (const float*)trk_in;
+  qp.f.hits = (const float*)hits;
+  qp.f.trk_out = (float*)trk_out;
+  qp.f.chi2 = chi2_out;
+  qp.f.dr = nullptr;
+  qp.f.nlay = q->nlay_lane;
+  qp.f.nblocks = q->nblocks;
+  qp.f.bsize = q->bsize;
+  qp.f.nlayer = q->nlayer;
+  qp.f.kfact = p2r_kfact_of(q->bz);
+  qp.items = q->items;
+  qp.n_items = q->n_items;
+  qp.counter = (int*)((char*)workspace + w.counter_off);
+  qp.t_start = start_ns;
+  qp.ev_remaining = (int*)((char*)workspace + w.remaining_off);
+  qp.ev_done = event_done_ns;
+  queue_init_kernel<<<(unsigned)((q->nevts + 255) / 256), 256, 0, st>>>(
+      q->event_block_offset, q->nevts, q->bsize / 32, qp.counter, qp.ev_remaining, start_ns);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    const int threads = q->block_threads > 0 ? q->block_threads : 128;
+    const int stages = q->stages > 0 ? q->stages : 4;
+    const bool fp64 = !(q->flags & P2R_FLAG_FP32_DET);
+    const bool chi2 = chi2_out != nullptr;
+    if (stages == 2)
+      e = chi2 ? (fp64 ? launch_queue_bs<2, true, true>(qp, threads, q->ctas_per_sm, st)
+                       : launch_queue_bs<2, true, false>(qp, threads, q->ctas_per_sm, st))
+               : (fp64 ? launch_queue_bs<2, false, true>(qp, threads, q->ctas_per_sm, st)
+                       : launch_queue_bs<2, false, false>(qp, threads, q->ctas_per_sm, st));
+    else
+      e = chi2 ? (fp64 ? launch_queue_bs<4, true, true>(qp, threads, q->ctas_per_sm, st)
+                       : launch_queue_bs<4, true, false>(qp, threads, q->ctas_per_sm, st))
+               : (fp64 ? launch_queue_bs<4, false, true>(qp, threads, q->ctas_per_sm, st)
+                       : launch_queue_bs<4, false, false>(qp, threads, q->ctas_per_sm, st));
+  }
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: launch failed: %s", who, cudaGetErrorString(e));
+  return p2r_clear_error();
+}
+
+}  // namespace
+
+struct p2r_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+int64_t p2r_queue_plan(const int64_t* host_event_block_offset, int64_t nevts, int32_t blocks_per_item,
+                       p2r_queue_item* host_items, int64_t capacity) {
+  if (!host_event_block_offset || nevts < 0 || blocks_per_item < 1)
+    return -p2r_set_error(P2R_ERR_INVALID, "p2r_queue_plan: bad arguments");
+  int64_t n = 0;
+  for (int64_t e = 0; e < nevts; ++e) {
+    const int64_t b0 = host_event_block_offset[e], b1 = host_event_block_offset[e + 1];
+    if (b1 < b0) return -p2r_set_error(P2R_ERR_QUEUE, "p2r_queue_plan: event offsets must not decrease");
+    for (int64_t b = b0; b < b1; b += blocks_per_item) {
+      if (host_items) {
+        if (n >= capacity) return -p2r_set_error(P2R_ERR_QUEUE, "p2r_queue_plan: item capacity exceeded");
+        host_items[n].event = (int32_t)e;
+        host_items[n].nblk = (int32_t)((b1 - b < blocks_per_item) ? (b1 - b) : blocks_per_item);
+        host_items[n].block0 = b;
+      }
+      ++n;
+    }
+  }
+  p2r_clear_error();
+  return n;
+}
+
+size_t p2r_queue_workspace_size(const p2r_queue* q) {
+  if (!q || q->nevts < 0) return 0;
+  return queue_ws(q->nevts).bytes;
+}
+
+int p2r_run_queue(const p2r_queue* q, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
+                  unsigned long long* event_done_ns, unsigned long long* start_ns, void* workspace, size_t ws_bytes,
+                  void* stream) {
+  return enqueue_queue(q, trk_in, hits, trk_out, chi2_out, event_done_ns, start_ns, workspace, ws_bytes,
+                       (cudaStream_t)stream, "p2r_run_queue");
+}
+
+int p2r_queue_graph_create(const p2r_queue* q, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
+                           unsigned long long* event_done_ns, unsigned long long* start_ns, void* workspace,
+                           size_t ws_bytes, p2r_graph** out) {
+  if (!out) return p2r_set_error(P2R_ERR_INVALID, "p2r_queue_graph_create: out is null");
+  *out = nullptr;
+  int rc = check_queue(q, "p2r_queue_graph_create");
+  if (rc) return rc;
+  cudaStream_t cs;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_queue_graph_create: %s", cudaGetErrorString(e));
+  p2r_graph* g = new (std::nothrow) p2r_graph();
+  if (!g) {
+    cudaStreamDestroy(cs);
+    return p2r_set_error(P2R_ERR_INVALID, "p2r_queue_graph_create: out of host memory");
+  }
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = enqueue_queue(q, trk_in, hits, trk_out, chi2_out, event_done_ns, start_ns, workspace, ws_bytes, cs,
+                       "p2r_queue_graph_create");
+    cudaError_t e2 = cudaStreamEndCapture(cs, &g->graph);
+    if (!rc && e2 != cudaSuccess) e = e2;
+  }
+  if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  cudaStreamDestroy(cs);
+  if (rc || e != cudaSuccess) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return rc ? rc : p2r_set_errorf(P2R_ERR_CUDA, "p2r_queue_graph_create: %s", cudaGetErrorString(e));
+  }
+  *out = g;
+  return p2r_clear_error();
+}
+
+int p2r_graph_launch(p2r_graph* g, void* stream) {
+  if (!g || !g->exec) return p2r_set_error(P2R_ERR_INVALID, "p2r_graph_launch: null graph");
+  cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_graph_launch: %s", cudaGetErrorString(e));
+  return p2r_clear_error();
+}
+
+int p2r_graph_destroy(p2r_graph* g) {
+  if (!g) return P2R_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return p2r_clear_error();
+}
+
+}  // extern "C"

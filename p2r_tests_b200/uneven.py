@@ -1,0 +1,116 @@
+"""Uneven batches through the persistent work-queue launch (p2r_run_queue) and its CUDA graph.
+
+`uneven_workload` builds the batched workload: events with log-normal track counts (blocks
+padded to bsize, padding lanes given zero layers) and uniform per-track layer counts, hits
+on nlayer_max cylinders. `Queue` holds the device-side description, the workspace and the
+per-event completion timestamps, and runs the launch directly or through a captured graph.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import CQueue, CQueueItem, P2RError, check, lib
+from .api import Config, _ptr, _stream, gen_params, generate_helix
+
+
+def lognormal_counts(nevts: int, median: float = 2000.0, sigma: float = 1.0, lo: int = 50, hi: int = 20000,
+                     seed: int = 7) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return np.clip(np.round(median * np.exp(sigma * rng.standard_normal(nevts))), lo, hi).astype(np.int64)
+
+
+def uneven_workload(ntrk_event, bsize: int = 32, nlayer_max: int = 25, lay_lo: int = 10, lay_hi: int = 25,
+                    bz: float = 3.8, seed: int = 20240002, r_first: float = 20.0, r_last: float = 100.0) -> dict:
+    """Host arrays of an uneven batch. Returns dict(trk, hit, nlay_lane, event_block_offset,
+    ntrk_event, nblocks, updates)."""
+    ntrk_event = np.asarray(ntrk_event, np.int64)
+    nb_event = (ntrk_event + bsize - 1) // bsize
+    off = np.zeros(len(ntrk_event) + 1, np.int64)
+    off[1:] = np.cumsum(nb_event)
+    nblocks = int(off[-1])
+    cfg = Config(bsize=bsize, nlayer=nlayer_max, nevts=1, nb=nblocks, bz=bz)
+    trk, hit = generate_helix(cfg, gen_params(bz=bz, seed=seed, r_first=r_first, r_last=r_last))
+    rng = np.random.default_rng(seed)
+    nlay = rng.integers(lay_lo, lay_hi + 1, nblocks * bsize).astype(np.int32)
+    # lanes past an event's track count are padding: no layers
+    lane_in_event = np.arange(nblocks * bsize) - np.repeat(off[:-1] * bsize, nb_event * bsize)
+    nlay[lane_in_event >= np.repeat(ntrk_event, nb_event * bsize)] = 0
+    return dict(trk=trk, hit=hit, nlay_lane=nlay, event_block_offset=off, ntrk_event=ntrk_event,
+                nblocks=nblocks, bsize=bsize, nlayer=nlayer_max, bz=bz, updates=int(nlay.sum()))
+
+
+def plan(event_block_offset: np.ndarray, blocks_per_item: int) -> np.ndarray:
+    """Work items (event, nblk, block0) as a structured numpy array."""
+    off = np.ascontiguousarray(event_block_offset, np.int64)
+    nevts = len(off) - 1
+    n = lib().p2r_queue_plan(off.ctypes.data, nevts, blocks_per_item, None, 0)
+    if n < 0:
+        raise P2RError(-n, lib().p2r_last_error_string().decode())
+    items = (CQueueItem * max(n, 1))()
+    m = lib().p2r_queue_plan(off.ctypes.data, nevts, blocks_per_item, ctypes.addressof(items), n)
+    if m < 0:
+        raise P2RError(-m, lib().p2r_last_error_string().decode())
+    dt = np.dtype([("event", np.int32), ("nblk", np.int32), ("block0", np.int64)])
+    return np.frombuffer(bytes(items), dtype=dt, count=n).copy()
+
+
+class Queue:
+    """Device description of an uneven batch for p2r_run_queue / p2r_queue_graph_create."""
+
+    def __init__(self, w: dict, blocks_per_item: int = 4, block_threads: int = 0, stages: int = 0,
+                 ctas_per_sm: int = 0, flags: int = 0, device="cuda"):
+        import torch
+        self.torch = torch
+        self.w = w
+        self.dev = torch.device(device)
+        items = plan(w["event_block_offset"], blocks_per_item)
+        self.n_items = len(items)
+        self.d_off = torch.from_numpy(w["event_block_offset"]).to(self.dev)
+        self.d_items = torch.from_numpy(items.view(np.uint8).copy()).to(self.dev)
+        self.d_nlay = torch.from_numpy(w["nlay_lane"]).to(self.dev)
+        self.nevts = len(w["ntrk_event"])
+        self.q = CQueue(w["bsize"], w["nlayer"], self.nevts, w["nblocks"], w["bz"], flags, block_threads, stages,
+                        ctas_per_sm, self.d_off.data_ptr(), self.d_items.data_ptr(), self.n_items,
+                        self.d_nlay.data_ptr())
+        ws = lib().p2r_queue_workspace_size(ctypes.byref(self.q))
+        self.ws = torch.empty(max(int(ws), 256), dtype=torch.uint8, device=self.dev)
+        self.done_ns = torch.zeros(self.nevts, dtype=torch.int64, device=self.dev)
+        self.start_ns = torch.zeros(1, dtype=torch.int64, device=self.dev)
+        self.graph = None
+
+    def run(self, trk_in, hits, trk_out, chi2=None, stream=None) -> None:
+        check(lib().p2r_run_queue(ctypes.byref(self.q), _ptr(trk_in), _ptr(hits), _ptr(trk_out), _ptr(chi2),
+                                  _ptr(self.done_ns), _ptr(self.start_ns), _ptr(self.ws), self.ws.numel(),
+                                  _stream(stream)))
+
+    def capture(self, trk_in, hits, trk_out, chi2=None) -> None:
+        """Captures the launch sequence into a CUDA graph (pointers are baked in)."""
+        self.release()
+        g = ctypes.c_void_p()
+        check(lib().p2r_queue_graph_create(ctypes.byref(self.q), _ptr(trk_in), _ptr(hits), _ptr(trk_out), _ptr(chi2),
+                                           _ptr(self.done_ns), _ptr(self.start_ns), _ptr(self.ws), self.ws.numel(),
+                                           ctypes.byref(g)))
+        self.graph = g
+
+    def replay(self, stream=None) -> None:
+        if self.graph is None:
+            raise P2RError(_lib.P2R_ERR_INVALID, "no graph captured")
+        check(lib().p2r_graph_launch(self.graph, _stream(stream)))
+
+    def release(self) -> None:
+        if self.graph is not None:
+            lib().p2r_graph_destroy(self.graph)
+            self.graph = None
+
+    def event_latency_ns(self) -> np.ndarray:
+        """Per-event completion time relative to the earliest CTA start of the last launch."""
+        return (self.done_ns - self.start_ns).cpu().numpy()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass

@@ -4,7 +4,8 @@ Reference gradient: torch autograd in FP64 over oracle/p2r_torch.py (pinned to t
 oracle and to central finite differences in tests/test_adjoint_cpu.py). Tolerance: each
 gradient within 1e-3 relative of the FP64 reference, relative to max(|g|, 1e-3 * the
 largest |g| of that gradient group) so components that are zero to rounding are judged
-against the group's scale.
+against the group's scale. The default adjoint runs in FP64; the FP32 mode
+(P2R_FLAG_ADJ_FP32) is held to its measured accuracy instead.
 """
 import numpy as np
 import pytest
@@ -62,7 +63,9 @@ def torch_reference(p2r, cfg, trk, hit, dr, g_trk, g_chi2, nlay=None):
                 dr=drt.grad.numpy(), bz=float(bz.grad), out_par=par.detach().numpy(), chi2=chi2.detach().numpy())
 
 
-def gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=5, nlay=None, per_event=False):
+def gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=5, nlay=None, per_event=False, fp32=False):
+    if fp32:
+        cfg = p2r.Config(**{**cfg.__dict__, "flags": cfg.flags | p2r.FLAG_ADJ_FP32})
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
     o = p2r.forward_backward(cfg, d(trk), d(hit), dr=d(dr), nlay_lane=None if nlay is None else d(nlay),
                              grad_trk_out=d(g_trk), grad_chi2=d(g_chi2), ckpt_stride=ckpt, per_event=per_event)
@@ -97,12 +100,21 @@ def test_adjoint_matches_fp64_reference(p2r, torch):
         e = grad_err(got[key], ref[key])
         report[key] = (float(np.quantile(e, 0.99)), float(e.max()))
     report["bz"] = float(grad_err([got["bz"]], [ref["bz"]])[0])
-    for key in ("par0", "hpos", "dr"):
-        assert report[key][0] < GRAD_RTOL, report
+    for key in ("par0", "cov0", "hpos", "hcov", "dr"):
+        assert report[key][1] < GRAD_RTOL, report  # every element
     assert report["bz"] < GRAD_RTOL, report
-    # covariance-side gradients: same bound at the 99th percentile
-    for key in ("cov0", "hcov"):
-        assert report[key][0] < GRAD_RTOL, report
+
+
+def test_fp32_adjoint_mode(p2r, torch):
+    """The FP32 instance of the same kernel: measured accuracy (not the 1e-3 bar): median
+    per-track gradient error ~1e-3, shared gradients (dr, Bz) within a few percent."""
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch)
+    ref = torch_reference(p2r, cfg, trk, hit, dr, g_trk, g_chi2)
+    got = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, fp32=True)
+    assert np.quantile(grad_err(got["par0"], ref["par0"]), 0.5) < 1e-2
+    assert np.quantile(grad_err(got["hpos"], ref["hpos"]), 0.5) < 1e-2
+    assert grad_err(got["dr"], ref["dr"]).max() < 0.1
+    assert grad_err([got["bz"]], [ref["bz"]])[0] < 0.1
 
 
 @pytest.mark.parametrize("ckpt", [1, 2, 4, 10])
@@ -115,9 +127,20 @@ def test_checkpoint_strides_agree(p2r, torch, ckpt):
     assert abs(other["bz"] - base["bz"]) <= 1e-5 * abs(base["bz"])
 
 
-def test_forward_outputs_match_plain_forward(p2r, torch):
+def test_forward_outputs_are_fp64_chain(p2r, oracle, torch):
+    """The FP64 kernel's forward outputs are the FP64 chain rounded to float."""
     cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch)
     got = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2)
+    f64 = oracle.run(trk, hit, 32, cfg.nlayer, 1, cfg.bz, "f64", dr=dr.astype(np.float64))
+    tp, tc, _ = parity.unpack(got["trk_out"], 32)
+    assert (parity.rel_par(tp, f64["par"]) < 1e-6).all()
+    assert (parity.rel_cov(tc, f64["cov"], f64["prior"]) < 1e-5).all()
+    assert (np.abs(got["chi2"] - f64["chi2"]) <= 1e-6 * np.maximum(np.abs(f64["chi2"]), 1)).all()
+
+
+def test_fp32_forward_outputs_match_plain_forward(p2r, torch):
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch)
+    got = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, fp32=True)
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
     out = torch.empty(trk.size, dtype=torch.float32, device="cuda")
     chi2 = torch.empty(cfg.ntracks, dtype=torch.float32, device="cuda")

@@ -147,7 +147,7 @@ def test_chained_step_parity_along_the_chain(p2r, oracle, torch):
         c1 = p2r.Config(bsize=32, nlayer=1, nevts=cfg.nevts, nb=cfg.nb, bz=cfg.bz)
         got = gpu_forward(p2r, torch, c1, state, h1)
         f64 = oracle.run(state, h1, 32, 1, 1, cfg.bz, "f64")
-        parity.assert_elementwise(got, want, f64["prior"], 32, f"step {l}")
+        parity.assert_step(got, want, f64["par"], f64["cov"], f64["prior"], 32, f"step {l}")
         state = want
 
 
@@ -174,12 +174,12 @@ def test_per_layer_calls_match_reference_steps(p2r, oracle, torch, mode):
         want = ref.run(inp, h1, cfg.nevts, cfg.nb, 1, chained=True)
         f64 = oracle.run(inp, h1, 32, 1, 1, cfg.bz, "f64")
         got = host(out)
-        parity.assert_elementwise(got, want, f64["prior"], 32, f"layer {l}")
+        parity.assert_step(got, want, f64["par"], f64["cov"], f64["prior"], 32, f"layer {l}")
         out.copy_(dev(torch, want))  # continue from the reference state (step parity)
         state = want
 
 
-def test_propagate_alone_matches_reference_block(p2r, torch):
+def test_propagate_alone_matches_reference_block(p2r, oracle, torch):
     """propagateToR alone (no update) against the reference's function on every block."""
     ref = ref_or_none(32, "kf")
     if ref is None:
@@ -198,9 +198,10 @@ def test_propagate_alone_matches_reference_block(p2r, torch):
             ob = tb.copy()  # the reference's propagateToR writes par and cov only; q stays
             ref.l.ref_propagate_block(tb.ctypes.data, hb.ctypes.data, ob.ctypes.data)
             want[b] = ob
-        _, wc, _ = parity.unpack(want, 32)
-        # no update: the output covariance itself is the conditioning scale
-        parity.assert_elementwise(got, want, wc, 32, f"propagate layer {l}")
+        h1 = slice_layer(hit, cfg.nblocks, cfg.nlayer, l, 32)
+        f64 = oracle.run(trk, h1, 32, 1, 2, cfg.bz, "f64")  # propagation only
+        # no update: the propagated covariance itself is the conditioning scale
+        parity.assert_step(got, want, f64["par"], f64["cov"], f64["prior"], 32, f"propagate layer {l}")
 
 
 # ---------------------------------------------------------------------------- internal consistency
@@ -275,15 +276,22 @@ def test_empty_and_single_block(p2r, torch):
 
 
 def test_chi2_and_radius_offsets_match_oracle(p2r, oracle, torch):
+    """chi2 and the radius offsets against the FP64 oracle, with the FP32 oracle as the yardstick:
+    chi2 is computed from residuals of ~10 um at radii up to 100 cm, where an FP32 position
+    carries ~8e-6 cm of rounding, so any FP32 chain has ~1e-3 (median) relative chi2 error."""
     cfg, trk, hit = helix(p2r, 2, 8)
     rng = np.random.default_rng(7)
     dr = rng.uniform(-0.01, 0.01, cfg.nlayer)  # +-100 um
     for mode in (0, 1):
         cfg.mode = mode
         out, chi2 = gpu_forward(p2r, torch, cfg, trk, hit, chi2=True, dr=dr.astype(np.float32))
-        f64 = oracle.run(trk, hit, 32, cfg.nlayer, mode, cfg.bz, "f64", dr=dr.astype(np.float32).astype(np.float64))
+        drd = dr.astype(np.float32).astype(np.float64)
+        f64 = oracle.run(trk, hit, 32, cfg.nlayer, mode, cfg.bz, "f64", dr=drd)
+        f32 = oracle.run(trk, hit, 32, cfg.nlayer, mode, cfg.bz, "f32", dr=drd)
         rel = np.abs(chi2 - f64["chi2"]) / np.maximum(np.abs(f64["chi2"]), 1.0)
-        assert np.quantile(rel, 0.99) < 1e-3, np.quantile(rel, [0.5, 0.99, 1])
+        rel32 = np.abs(f32["chi2"] - f64["chi2"]) / np.maximum(np.abs(f64["chi2"]), 1.0)
+        for q in (0.5, 0.9, 0.99):
+            assert np.quantile(rel, q) <= 2 * np.quantile(rel32, q) + 1e-6, (q, np.quantile(rel, q), np.quantile(rel32, q))
         tp = parity.unpack(out, 32)[0]
         assert np.quantile(parity.rel_par(tp, f64["par"]), 0.99) < parity.PAR_RTOL
 

@@ -1,0 +1,163 @@
+"""Uneven batches: work-item planning (CPU) and the persistent queue launch (GPU)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from tests import parity
+
+
+def test_plan_splits_events_in_order(p2r):
+    off = np.array([0, 5, 5, 12, 13], np.int64)  # event 1 is empty
+    items = p2r.plan(off, 3)
+    assert [tuple(x) for x in items] == [(0, 3, 0), (0, 2, 3), (2, 3, 5), (2, 3, 8), (2, 1, 11), (3, 1, 12)]
+    assert sum(int(x["nblk"]) for x in items) == 13
+
+
+def test_plan_rejects_bad_offsets(p2r):
+    l = p2r.lib()
+    off = np.array([0, 4, 2], np.int64)
+    assert l.p2r_queue_plan(off.ctypes.data, 2, 2, None, 0) < 0
+    off = np.array([0, 4, 8], np.int64)
+    assert l.p2r_queue_plan(off.ctypes.data, 2, 0, None, 0) < 0
+    buf = (p2r._lib.CQueueItem * 1)()
+    assert l.p2r_queue_plan(off.ctypes.data, 2, 2, ctypes.addressof(buf), 1) < 0  # capacity
+
+
+def test_queue_rejects_bad_description(p2r):
+    l = p2r.lib()
+    q = p2r._lib.CQueue(48, 25, 1, 1, 3.8, 0, 0, 0, 0, None, None, 0, None)  # bsize not a multiple of 32
+    assert l.p2r_run_queue(ctypes.byref(q), None, None, None, None, None, None, None, 0, None) == p2r._lib.P2R_ERR_QUEUE
+    q = p2r._lib.CQueue(32, 25, 1, 4, 3.8, 0, 0, 0, 0, None, None, 1, None)  # blocks but no arrays
+    assert l.p2r_run_queue(ctypes.byref(q), None, None, None, None, None, None, None, 0, None) == p2r._lib.P2R_ERR_QUEUE
+
+
+def test_uneven_workload_padding(p2r):
+    w = p2r.uneven_workload(np.array([33, 64, 1, 50]), bsize=32)
+    assert list(w["event_block_offset"]) == [0, 2, 4, 5, 7]
+    nl = w["nlay_lane"].reshape(-1, 32)
+    assert (nl[1, 1:] == 0).all() and (nl[1, 0] > 0)  # event 0: 33 tracks -> 1 live lane in block 1
+    assert (nl[4, 1:] == 0).all()                     # event 2: 1 track
+    assert ((nl[0] >= 10) & (nl[0] <= 25)).all()
+    assert w["updates"] == int(nl.sum())
+
+
+# ------------------------------------------------------------------------------- GPU
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return t
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
+
+
+@pytest.fixture(scope="module")
+def small_batch(p2r):
+    return p2r.uneven_workload(p2r.lognormal_counts(24, median=150, sigma=1.0, lo=5, hi=2000, seed=3), bsize=32)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("g", [1, 4, 16])
+def test_queue_matches_masked_forward(p2r, torch, small_batch, g):
+    w = small_batch
+    q = p2r.Queue(w, blocks_per_item=g)
+    t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
+    out = torch.empty_like(t)
+    q.run(t, h, out)
+    cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"])
+    ref = torch.empty_like(t)
+    p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
+    torch.cuda.synchronize()
+    parity.assert_same_arithmetic(out.cpu().numpy(), ref.cpu().numpy(), 32, f"queue G={g} vs masked forward")
+    lat = q.event_latency_ns()
+    assert (lat > 0).all() and (lat < 10_000_000_000).all()
+
+
+@pytest.mark.gpu
+def test_queue_granularity_bit_identical(p2r, torch, small_batch):
+    w = small_batch
+    t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
+    outs = []
+    for g in (1, 3, 64):
+        o = torch.empty_like(t)
+        p2r.Queue(w, blocks_per_item=g).run(t, h, o)
+        outs.append(o.cpu().numpy().view(np.uint32))
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+
+
+@pytest.mark.gpu
+def test_queue_matches_reference(p2r, oracle, torch, small_batch):
+    from oracle.oracle import RefTBB, ref_available
+    if not ref_available(32, "kf"):
+        pytest.skip("reference build not present")
+    w = small_batch
+    ref = RefTBB(32, "kf")
+    ref.set_bz(w["bz"])
+    want = ref.run_masked(w["trk"], w["hit"], w["nlayer"], w["nlay_lane"])
+    t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
+    out = torch.empty_like(t)
+    p2r.Queue(w, blocks_per_item=4).run(t, h, out)
+    torch.cuda.synchronize()
+    f64 = oracle.run(w["trk"], w["hit"], 32, w["nlayer"], 1, w["bz"], "f64", nlay_lane=w["nlay_lane"])
+    got = out.cpu().numpy()
+    live = w["nlay_lane"] > 0
+    sel = lambda a: a.reshape(-1, 28, 32).transpose(0, 2, 1).reshape(-1, 28)[live].reshape(-1, 1, 28).transpose(0, 2, 1).reshape(-1)
+    # compare live tracks only (padding lanes keep their input), as 1-lane blocks
+    parity.assert_accuracy_parity(sel(got), sel(want), f64["par"][live], f64["cov"][live], f64["prior"][live], 1,
+                                  "queue vs reference (masked)")
+    # padding lanes are returned unchanged
+    pad = ~live
+    a = got.reshape(-1, 28, 32).transpose(0, 2, 1).reshape(-1, 28)[pad]
+    b = w["trk"].reshape(-1, 28, 32).transpose(0, 2, 1).reshape(-1, 28)[pad]
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_queue_graph_replay(p2r, torch, small_batch):
+    w = small_batch
+    q = p2r.Queue(w, blocks_per_item=2)
+    t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
+    direct = torch.empty_like(t)
+    q.run(t, h, direct)
+    out = torch.zeros_like(t)
+    chi2 = torch.zeros(w["nblocks"] * 32, dtype=torch.float32, device="cuda")
+    q.capture(t, h, out, chi2)
+    for _ in range(3):
+        out.zero_()
+        q.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), direct.cpu().numpy().view(np.uint32))
+    lat = q.event_latency_ns()
+    assert (lat > 0).all()
+    assert np.isfinite(chi2.cpu().numpy()).all()
+    q.release()
+
+
+@pytest.mark.gpu
+def test_queue_empty_events_and_tiny(p2r, torch):
+    w = p2r.uneven_workload(np.array([0, 1, 0, 40, 0]), bsize=32)
+    q = p2r.Queue(w, blocks_per_item=1)
+    t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
+    out = torch.empty_like(t)
+    q.run(t, h, out)
+    torch.cuda.synchronize()
+    lat = q.event_latency_ns()
+    assert (lat[[1, 3]] > 0).all()  # events with blocks complete; empty events have no slices
+    assert np.isfinite(p2r.tracks_par(out.cpu().numpy().reshape(-1, 28, 32))[w["nlay_lane"] > 0]).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("bs", [64, 128])
+def test_queue_wide_blocks(p2r, torch, bs):
+    w = p2r.uneven_workload(p2r.lognormal_counts(6, median=300, lo=5, hi=2000, seed=5), bsize=bs)
+    t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
+    out, ref = torch.empty_like(t), torch.empty_like(t)
+    p2r.Queue(w, blocks_per_item=2).run(t, h, out)
+    cfg = p2r.Config(bsize=bs, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"])
+    p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
+    torch.cuda.synchronize()
+    parity.assert_same_arithmetic(out.cpu().numpy(), ref.cpu().numpy(), bs, f"queue bsize {bs}")
