@@ -109,14 +109,16 @@ def assert_accuracy_parity(test_trk, ref_trk, f64_par, f64_cov, prior, bsize, wh
 def assert_same_arithmetic(a, b, bs, what):
     """Two launches of the same arithmetic: q bit-equal, values equal up to the rounding of
     differently contracted FMAs (separately compiled kernel variants may fuse a*b+c in
-    different places), i.e. a few float ulps per layer, checked as a relative bound."""
+    different places). Most tracks come out bit-identical; the chained filter amplifies the
+    rest, so the bound is the FP32 accuracy level itself (PAR_RTOL at the 99.9th percentile)."""
     ap, ac, aq = unpack(a, bs)
     bp, bc, bq = unpack(b, bs)
     assert np.array_equal(aq, bq), what
     ep = np.abs(ap - bp) / np.maximum(np.abs(bp), PAR_FLOOR)
     ec = np.abs(ac - bc) / np.maximum(np.abs(bc), cov_scale(bc))
-    assert np.quantile(ep, 0.999) < 1e-5 and ep.max() < 1e-3, (what, np.quantile(ep, [0.5, 0.999, 1]))
-    assert np.quantile(ec, 0.999) < 1e-4 and ec.max() < 1e-2, (what, np.quantile(ec, [0.5, 0.999, 1]))
+    assert np.quantile(ep, 0.5) == 0 and np.quantile(ep, 0.999) < PAR_RTOL and ep.max() < 1e-3, \
+        (what, np.quantile(ep, [0.5, 0.999, 1]))
+    assert np.quantile(ec, 0.999) < COV_RTOL and ec.max() < 1e-1, (what, np.quantile(ec, [0.5, 0.999, 1]))
 
 
 def assert_step(test_trk, ref_trk, f64_par, f64_cov, prior, bsize, what=""):
