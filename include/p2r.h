@@ -213,6 +213,24 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
                          double* grad_bz, double* grad_dr_event, double* grad_bz_event, int32_t ckpt_stride,
                          void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of p2r_forward_backward (no counterpart in the reference): the
+ * same arguments without a workspace; the workspace is a fixed 8 MiB device array inside the
+ * library, held by every GPU that loads it until the process exits. For callers that cannot
+ * allocate device memory when they need gradients: code running while another framework
+ * captures a CUDA graph, event loops that forbid allocation after start-up, plugin hosts whose
+ * device memory belongs to the host framework's pool. Batches whose workspace
+ * (p2r_forward_backward_workspace_size) exceeds 8 MiB are rejected with P2R_ERR_WORKSPACE
+ * (about 3 M tracks at 20 layers, fewer with more layers or events). The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress, with that device
+ * current); make that first call before any stream capture. Every call shares the array:
+ * calls that overlap on the GPU race. Nothing in it needs clearing (each call writes
+ * everything it reads). No cudaMalloc / cudaFree. */
+int p2r_forward_backward_noalloc(const p2r_config* cfg, const void* trk_in, const void* hits, const float* dr,
+                                 const int32_t* nlay_lane, void* trk_out, float* chi2_out, const void* grad_trk_out,
+                                 const float* grad_chi2, void* grad_trk_in, void* grad_hits, double* grad_dr,
+                                 double* grad_bz, double* grad_dr_event, double* grad_bz_event, int32_t ckpt_stride,
+                                 void* stream);
+
 /* ---------------------------------------------------------------- autotuning
  * Times p2r_forward on the caller's arrays for every (threads[i], stages[j]) pair
  * (CUDA events on `stream`, one warm-up launch then `reps` launches each) and reports the

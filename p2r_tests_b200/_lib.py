@@ -111,6 +111,8 @@ SIGNATURES = {
     "p2r_forward_host": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "p2r_fp32_fma_probe": (ctypes.c_int, [_i64, _i32, _i32, _vp, _vp]),
     "p2r_forward_backward_workspace_size": (ctypes.c_size_t, [_cfgp]),
+    "p2r_forward_backward_noalloc": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                    _vp, _vp, _vp, _i32, _vp]),
     "p2r_queue_plan": (ctypes.c_int64, [_vp, _i64, _i32, _vp, _i64]),
     "p2r_autotune_forward": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _i32, _vp, _i32, _i32, _vp, _vp]),
     "p2r_queue_workspace_size": (ctypes.c_size_t, [_vp]),

@@ -373,3 +373,73 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free variant
+// Some callers cannot allocate device memory at the point where they need gradients:
+// code running while another framework captures a CUDA graph (cudaMalloc is not allowed
+// during stream capture), online / trigger-style event loops that forbid allocation after
+// start-up (unbounded latency and pool fragmentation), and plugin hosts whose device
+// memory is entirely owned by the host framework's pool. For them the workspace of
+// p2r_forward_backward lives in this fixed device array instead. Every GPU that loads the
+// library holds the array until the process exits.
+#include <mutex>
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB per GPU
+static __device__ __align__(256) unsigned char g_fwdbwd_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_scratch_mu;
+void* g_scratch_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_fwdbwd_scratch on the current device. In host code the array's name
+// is only a host-side stand-in, so the address is looked up once per device (with that
+// device current) and cached.
+int scratch_address(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess)
+    return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_backward_noalloc: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "p2r_forward_backward_noalloc: device %d", dev);
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_fwdbwd_scratch);
+    if (e != cudaSuccess || !p)
+      return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_backward_noalloc: scratch address: %s",
+                            cudaGetErrorString(e));
+    g_scratch_ptr[dev] = p;
+  }
+  *out = g_scratch_ptr[dev];
+  return P2R_OK;
+}
+
+}  // namespace
+
+extern "C" int p2r_forward_backward_noalloc(const p2r_config* cfg, const void* trk_in, const void* hits,
+                                            const float* dr, const int32_t* nlay_lane, void* trk_out,
+                                            float* chi2_out, const void* grad_trk_out, const float* grad_chi2,
+                                            void* grad_trk_in, void* grad_hits, double* grad_dr, double* grad_bz,
+                                            double* grad_dr_event, double* grad_bz_event, int32_t ckpt_stride,
+                                            void* stream) {
+  int rc = p2r_check_config(cfg, "p2r_forward_backward_noalloc");
+  if (rc) return rc;
+  const size_t need = layout_of(cfg).total_bytes;
+  if (need > kNoAllocScratchBytes)
+    return p2r_set_errorf(P2R_ERR_WORKSPACE,
+                          "p2r_forward_backward_noalloc: this batch needs %zu bytes of scratch; the allocation-free "
+                          "entry point has a fixed %zu bytes per GPU (about (tracks/32)*(nlayer+1)*4 + "
+                          "nevts*(nlayer+1)*8 bytes are used): split the batch or pass a workspace to "
+                          "p2r_forward_backward",
+                          need, kNoAllocScratchBytes);
+  void* ws = nullptr;
+  if ((rc = scratch_address(&ws))) return rc;
+  // Nothing in the scratch must start at zero: the kernel writes every partial it reads
+  // and the reductions write every sum. Calls that overlap on the GPU (other streams or
+  // threads) share the array and race.
+  return p2r_forward_backward(cfg, trk_in, hits, dr, nlay_lane, trk_out, chi2_out, grad_trk_out, grad_chi2,
+                              grad_trk_in, grad_hits, grad_dr, grad_bz, grad_dr_event, grad_bz_event, ckpt_stride,
+                              ws, kNoAllocScratchBytes, stream);
+}
