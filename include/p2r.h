@@ -252,6 +252,18 @@ int p2r_autotune_forward(const p2r_config* cfg, const void* trk_in, const void* 
  * = 64 * iters * blocks * threads. out: blocks*threads floats. threads: 32..256. */
 int p2r_fp32_fma_probe(int64_t iters, int32_t blocks, int32_t threads, float* out, void* stream);
 
+/* The division / square-root build of the hot path (no reference counterpart; the reference
+ * takes whatever its compiler flags give). P2R_MATH_REFINED: hardware reciprocal and
+ * reciprocal square root refined by one Newton-Raphson step (the default build);
+ * P2R_MATH_IEEE: correctly rounded; P2R_MATH_FAST: the approximations alone. */
+enum p2r_math { P2R_MATH_REFINED = 0, P2R_MATH_IEEE = 1, P2R_MATH_FAST = 2 };
+int32_t p2r_math_variant(void);
+
+/* Evaluates the hot path's own division and square root elementwise on the device:
+ * quot[i] = a[i] / b[i], root[i] = sqrt(a[i]), for measuring their error against the
+ * correctly rounded results. Device pointers, n >= 0. */
+int p2r_math_check(int64_t n, const float* a, const float* b, float* quot, float* root, void* stream);
+
 /* ---------------------------------------------------------------- host-side helpers */
 
 /* Parameters of the synthetic helix generator (p2r_gen_helix).

@@ -25,6 +25,7 @@ MODE_CHAINED = 1
 FLAG_FP32_DET = 0x1
 FLAG_NO_STAGING = 0x2
 FLAG_ADJ_FP32 = 0x4
+MATH_REFINED, MATH_IEEE, MATH_FAST = 0, 1, 2
 
 
 class P2RError(RuntimeError):
@@ -110,6 +111,8 @@ SIGNATURES = {
     "p2r_count_nonfinite": (ctypes.c_int, [_vp, _i64, _i32, _vp, _vp]),
     "p2r_forward_host": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "p2r_fp32_fma_probe": (ctypes.c_int, [_i64, _i32, _i32, _vp, _vp]),
+    "p2r_math_variant": (ctypes.c_int32, []),
+    "p2r_math_check": (ctypes.c_int, [_i64, _vp, _vp, _vp, _vp, _vp]),
     "p2r_forward_backward_workspace_size": (ctypes.c_size_t, [_cfgp]),
     "p2r_forward_backward_noalloc": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                                     _vp, _vp, _vp, _i32, _vp]),

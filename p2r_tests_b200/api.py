@@ -153,6 +153,19 @@ def fp32_fma_probe(out, iters: int, blocks: int, threads: int = 256, stream=None
     return 64 * iters * blocks * threads
 
 
+def math_variant() -> str:
+    """Which division / square-root build the library is: "refined", "ieee" or "fast"."""
+    return {_lib.MATH_REFINED: "refined", _lib.MATH_IEEE: "ieee", _lib.MATH_FAST: "fast"}[lib().p2r_math_variant()]
+
+
+def math_check(a, b, stream=None):
+    """The hot path's own a / b and sqrt(a) on the device (float32 tensors of one size)."""
+    import torch
+    quot, root = torch.empty_like(a), torch.empty_like(a)
+    check(lib().p2r_math_check(a.numel(), _ptr(a), _ptr(b), _ptr(quot), _ptr(root), _stream(stream)))
+    return quot, root
+
+
 def count_nonfinite(trk, nblocks: int, bsize: int, stream=None) -> int:
     import torch
     cnt = torch.zeros(1, dtype=torch.int64, device=trk.device)

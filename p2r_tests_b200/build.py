@@ -85,6 +85,26 @@ def build_library(force: bool = False, verbose_ptxas: bool = False, quiet: bool 
     return LIB
 
 
+DRIVER_SRC = PKG / "driver" / "p2r_driver.cpp"
+DRIVER = PKG / "p2r_driver"
+
+
+def build_driver(force: bool = False) -> Path:
+    """The C++ driver program (the reference's main over the C ABI), linked to the library."""
+    lib = build_library()
+    if DRIVER.exists() and not force and DRIVER.stat().st_mtime >= max(DRIVER_SRC.stat().st_mtime,
+                                                                        lib.stat().st_mtime):
+        return DRIVER
+    cuda = cuda_home()
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", "-I" + str(ROOT / "include"),
+           "-I" + str(cuda / "include"), str(DRIVER_SRC), "-o", str(DRIVER), "-L" + str(PKG), "-lp2r_b200",
+           "-L" + str(cuda / "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + str(cuda / "lib64")]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"driver build failed: {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+    return DRIVER
+
+
 def build_oracle() -> None:
     """Builds oracle/_build (always) and oracle/_ref (only where the reference checkout exists)."""
     make = shutil.which("make")
@@ -98,6 +118,7 @@ def build_oracle() -> None:
 
 if __name__ == "__main__":
     build_library(force="--force" in sys.argv, verbose_ptxas="-v" in sys.argv, quiet=False)
+    build_driver(force="--force" in sys.argv)
     if "--oracle" in sys.argv:
         build_oracle()
     print(LIB)

@@ -77,7 +77,6 @@ struct PropTape {
   T D, dDdx, dDdy, dDdipt, dDdphi;
   T alpha, dadx, dady, dadipt, dadphi, sa, ca, omc, cT, sT, isT;
   T J00, J01, J03, J04, J10, J11, J13, J14, J20, J21, J23, J24, J25, J40, J41, J43, J44;
-  T T0[6], T1[6], T2[6], T4[6];  // rows 0, 1, 2, 4 of J*C
 };
 
 // propagateToR of (ip, ic) to radius r with k = q*kfact, kinv = 1/k, recording the tape.
@@ -159,22 +158,25 @@ P2R_UNROLL
   t.J41 = dady;
   t.J43 = dadipt;
   t.J44 = T(1) + dadphi;
+  // rows 0, 1, 2, 4 of J*C (rows 3 and 5 are rows 3 and 5 of C); not kept on the tape:
+  // the reverse forms J-bar as (S J) C instead of S (J C)
+  T T0[6], T1[6], T2[6], T4[6];
 P2R_UNROLL
   for (int j = 0; j < 6; ++j) {
     const T c0 = ic[S6(0, j)], c1 = ic[S6(1, j)], c2 = ic[S6(2, j)], c3 = ic[S6(3, j)], c4 = ic[S6(4, j)],
             c5 = ic[S6(5, j)];
-    t.T0[j] = t.J00 * c0 + t.J01 * c1 + t.J03 * c3 + t.J04 * c4;
-    t.T1[j] = t.J10 * c0 + t.J11 * c1 + t.J13 * c3 + t.J14 * c4;
-    t.T2[j] = t.J20 * c0 + t.J21 * c1 + c2 + t.J23 * c3 + t.J24 * c4 + t.J25 * c5;
-    t.T4[j] = t.J40 * c0 + t.J41 * c1 + t.J43 * c3 + t.J44 * c4;
+    T0[j] = t.J00 * c0 + t.J01 * c1 + t.J03 * c3 + t.J04 * c4;
+    T1[j] = t.J10 * c0 + t.J11 * c1 + t.J13 * c3 + t.J14 * c4;
+    T2[j] = t.J20 * c0 + t.J21 * c1 + c2 + t.J23 * c3 + t.J24 * c4 + t.J25 * c5;
+    T4[j] = t.J40 * c0 + t.J41 * c1 + t.J43 * c3 + t.J44 * c4;
   }
-  // C' = (J C) J^T, lower triangle; rows 3 and 5 of J C are rows 3 and 5 of C
+  // C' = (J C) J^T, lower triangle
 P2R_UNROLL
   for (int i = 0; i < 6; ++i) {
     T Ti[6];
 P2R_UNROLL
     for (int j = 0; j < 6; ++j)
-      Ti[j] = i == 0 ? t.T0[j] : i == 1 ? t.T1[j] : i == 2 ? t.T2[j] : i == 4 ? t.T4[j] : ic[S6(i, j)];
+      Ti[j] = i == 0 ? T0[j] : i == 1 ? T1[j] : i == 2 ? T2[j] : i == 4 ? T4[j] : ic[S6(i, j)];
     oc[S6(i, 0)] = Ti[0] * t.J00 + Ti[1] * t.J01 + Ti[3] * t.J03 + Ti[4] * t.J04;
     if (i >= 1) oc[S6(i, 1)] = Ti[0] * t.J10 + Ti[1] * t.J11 + Ti[3] * t.J13 + Ti[4] * t.J14;
     if (i >= 2)
@@ -212,32 +214,12 @@ P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], 
   T ptb = zb * k * alpha * cT * isT;
   T isTb = zb * k * alpha * cT * pt;
 
-  // ---- C' = J C J^T: S = Gbar + Gbar^T, Jbar = S (J C), cbar = packed(J^T S J)
+  // ---- C' = J C J^T: S = Gbar + Gbar^T, Jbar = S (J C) = (S J) C, cbar = packed(J^T S J)
   T S[6][6];
 P2R_UNROLL
   for (int i = 0; i < 6; ++i)
 P2R_UNROLL
     for (int j = 0; j < 6; ++j) S[i][j] = i == j ? T(2) * cb_out[S6(i, i)] : cb_out[S6(i, j)];
-  T Tf[6][6];
-P2R_UNROLL
-  for (int j = 0; j < 6; ++j) {
-    Tf[0][j] = t.T0[j];
-    Tf[1][j] = t.T1[j];
-    Tf[2][j] = t.T2[j];
-    Tf[3][j] = ic[S6(3, j)];
-    Tf[4][j] = t.T4[j];
-    Tf[5][j] = ic[S6(5, j)];
-  }
-  auto ST = [&](int a, int b) {
-    T s = 0;
-P2R_UNROLL
-    for (int c = 0; c < 6; ++c) s += S[a][c] * Tf[c][b];
-    return s;
-  };
-  const T J00b = ST(0, 0), J01b = ST(0, 1), J03b = ST(0, 3), J04b = ST(0, 4);
-  const T J10b = ST(1, 0), J11b = ST(1, 1), J13b = ST(1, 3), J14b = ST(1, 4);
-  const T J20b = ST(2, 0), J21b = ST(2, 1), J23b = ST(2, 3), J24b = ST(2, 4), J25b = ST(2, 5);
-  const T J40b = ST(4, 0), J41b = ST(4, 1), J43b = ST(4, 3), J44b = ST(4, 4);
   // W = S J, M = J^T W
   T W[6][6];
 P2R_UNROLL
@@ -261,6 +243,18 @@ P2R_UNROLL
 P2R_UNROLL
     for (int i = j; i < 6; ++i) cb_in[S6(i, j)] = i == j ? T(0.5f) * M[i] : M[i];
   }
+
+  // Jbar = W C at the non-trivial entries of J
+  auto WC = [&](int a, int b) {
+    T s = 0;
+P2R_UNROLL
+    for (int c = 0; c < 6; ++c) s += W[a][c] * ic[S6(c, b)];
+    return s;
+  };
+  const T J00b = WC(0, 0), J01b = WC(0, 1), J03b = WC(0, 3), J04b = WC(0, 4);
+  const T J10b = WC(1, 0), J11b = WC(1, 1), J13b = WC(1, 3), J14b = WC(1, 4);
+  const T J20b = WC(2, 0), J21b = WC(2, 1), J23b = WC(2, 3), J24b = WC(2, 4), J25b = WC(2, 5);
+  const T J40b = WC(4, 0), J41b = WC(4, 1), J43b = WC(4, 3), J44b = WC(4, 4);
 
   // ---- Jacobian entries -> their inputs
   const T U = cP * ca - sP * sa, V = sP * ca + cP * sa, w = ipt * dadipt;

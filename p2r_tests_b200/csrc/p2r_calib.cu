@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "p2r_internal.h"
+#include "p2r_math.cuh"
 
 namespace {
 
@@ -28,7 +29,38 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(long long iters, float* 
   out[blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
 }
 
+// The hot path's own division and square root (p2r::fdiv, p2r::fsqrt) over caller arrays,
+// so their error against the correctly rounded results can be measured.
+__global__ void math_check_kernel(long long n, const float* __restrict__ a, const float* __restrict__ b,
+                                  float* __restrict__ quot, float* __restrict__ root) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    quot[i] = p2r::fdiv(a[i], b[i]);
+    root[i] = p2r::fsqrt(a[i]);
+  }
+}
+
 }  // namespace
+
+extern "C" int32_t p2r_math_variant(void) {
+#if defined(P2R_FAST_MATH)
+  return P2R_MATH_FAST;
+#elif defined(P2R_IEEE_MATH)
+  return P2R_MATH_IEEE;
+#else
+  return P2R_MATH_REFINED;
+#endif
+}
+
+extern "C" int p2r_math_check(int64_t n, const float* a, const float* b, float* quot, float* root, void* stream) {
+  if (n < 0 || (n > 0 && (!a || !b || !quot || !root)))
+    return p2r_set_error(P2R_ERR_INVALID, "p2r_math_check: bad arguments");
+  if (n == 0) return p2r_clear_error();
+  const long long blocks = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
+  math_check_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(n, a, b, quot, root);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_math_check: %s", cudaGetErrorString(e));
+  return p2r_clear_error();
+}
 
 // FLOPs per launch = 2 * 32 * iters * blocks * threads (4 unrolled rounds of 8 chains).
 extern "C" int p2r_fp32_fma_probe(int64_t iters, int32_t blocks, int32_t threads, float* out, void* stream) {

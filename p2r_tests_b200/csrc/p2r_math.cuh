@@ -19,15 +19,46 @@ namespace p2r {
 // packed lower-triangle index of a symmetric 6x6 (TBB:46-54)
 __host__ __device__ constexpr int S6(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
 
-// Division and square root. With P2R_FAST_MATH defined they are the hardware
-// approximations (div.approx / sqrt.approx, about 2 ulp) instead of the IEEE-rounded
-// sequences; every other operation is unchanged.
-#ifdef P2R_FAST_MATH
+// Division and square root, three builds:
+//  default            the hardware approximations (rcp.approx, rsqrt.approx) refined by one
+//                     Newton-Raphson step each (the textbook iteration, e.g. Markstein,
+//                     IBM J. Res. Dev. 34(1), 1990): y <- y + y (1 - b y) for 1/b, a/b = a y;
+//                     for sqrt(x), r ~ 1/sqrt(x), s = x r, s <- s + (r/2)(x - s s). Within
+//                     about an ulp of the rounded quotient / root (p2r_math_check measures it),
+//                     without the special-case paths of a correctly rounded sequence: the
+//                     arguments here are finite and normal and, for sqrt, positive
+//  P2R_IEEE_MATH      IEEE-rounded (a / b, sqrtf)
+//  P2R_FAST_MATH      the approximations alone (div.approx / sqrt.approx, about 2 ulp)
+// Every other operation is the same in all three.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+#if defined(P2R_FAST_MATH)
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ float fsqrt(float x) {
   float r;
   asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
+}
+#elif !defined(P2R_IEEE_MATH)
+#define P2R_REFINED_MATH 1
+__device__ __forceinline__ float frcp(float b) {
+  const float y = rcp_approx(b);
+  return fmaf(y, fmaf(-b, y, 1.f), y);
+}
+__device__ __forceinline__ float fdiv(float a, float b) { return a * frcp(b); }
+__device__ __forceinline__ float fsqrt(float x) {
+  if (!(x > 0.f)) return sqrtf(x);
+  const float r = rsqrt_approx(x);
+  const float s = x * r;
+  return fmaf(0.5f * r, fmaf(-s, s, x), s);
 }
 #else
 __device__ __forceinline__ float fdiv(float a, float b) { return a / b; }
@@ -179,7 +210,7 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
 template <bool kFp64Det, bool kChi2>
 __device__ __forceinline__ float kalman_update(float (&p)[6], float (&c)[21], const float (&hp)[3],
                                                const float (&hc)[6], float rhit) {
-#ifdef P2R_FAST_MATH
+#if defined(P2R_FAST_MATH) || defined(P2R_REFINED_MATH)
   const float inv2r = fdiv(0.5f, rhit);
   const float rotT00 = -(hp[1] + p[1]) * inv2r;
   const float rotT01 = (hp[0] + p[0]) * inv2r;

@@ -5,8 +5,8 @@ oracle/Makefile):  make -C oracle ref && python tests/golden/make_golden.py
 
 Everything here comes from the reference's CPU path (src/propagate-tor-test_tbb.cpp)
 compiled unmodified by oracle/ref_harness.cpp:
-  fixture.npz          the seed track and 22 hits of src/input_track.h in the order the
-                       reference's main uses them (TBB:818-820)
+  fixture.npz/.txt     the seed track and 22 hits of src/input_track.h in the order the
+                       reference's main uses them (TBB:818-820); .txt for the C++ driver
   ref_fixture_b{B}.npz for bsize B in 32/64/128: the reference's own generated inputs
                        (prepareTracks/prepareHits, TBB:243-293; inputs stored for B=32 only,
                        SHA-256 digests for all) and its outputs in restart mode (TBB:873-926)
@@ -46,6 +46,13 @@ def main() -> None:
     r32 = RefTBB(32, "v3")
     par, cov, q, hits = r32.fixture_raw()
     np.savez_compressed(HERE / "fixture.npz", par=par, cov=cov, q=np.int32(q), hits=hits)
+    # the same numbers as text, the input format of the C++ driver (--input fixture FILE)
+    with open(HERE / "fixture.txt", "w") as f:
+        f.write(" ".join(repr(float(x)) for x in par) + "\n")
+        f.write(" ".join(repr(float(x)) for x in cov) + "\n")
+        f.write(f"{q}\n")
+        for h in hits:
+            f.write(" ".join(repr(float(x)) for x in h) + "\n")
 
     for bs in (32, 64, 128):
         r = RefTBB(bs, "v3")
