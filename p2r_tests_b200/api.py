@@ -147,9 +147,10 @@ def forward_host(cfg: Config, host_trk_in: np.ndarray, host_hits: np.ndarray, ho
                                  nchunks, _stream(stream)))
 
 
-def fp32_fma_probe(out, iters: int, blocks: int, threads: int = 256, stream=None) -> int:
-    """Launches the FP32 FMA probe; returns the FLOPs it performs."""
-    check(lib().p2r_fp32_fma_probe(iters, blocks, threads, _ptr(out), _stream(stream)))
+def fp32_fma_probe(out, iters: int, blocks: int, threads: int = 256, stream=None, packed: bool = False) -> int:
+    """Launches the FP32 FMA probe (packed: the f32x2 form); returns the FLOPs it performs."""
+    fn = lib().p2r_fp32x2_fma_probe if packed else lib().p2r_fp32_fma_probe
+    check(fn(iters, blocks, threads, _ptr(out), _stream(stream)))
     return 64 * iters * blocks * threads
 
 

@@ -1,7 +1,7 @@
 // FP32 FMA throughput probe: the measured denominator of the hot path's compute roofline.
 // Each thread advances 8 independent FMA chains (enough independent work to cover the
 // FMA latency at full occupancy) for `iters` iterations; the result is stored so nothing
-// is eliminated. FLOPs per launch = 2 * 8 * iters * blocks * threads.
+// is eliminated. FLOPs per launch = 2 * 32 * iters * blocks * threads (8 chains, 4 rounds).
 #include <cuda_runtime.h>
 
 #include "p2r_internal.h"
@@ -29,6 +29,35 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(long long iters, float* 
   out[blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
 }
 
+// The same FLOPs with sm_100's packed f32x2 FMA (two lanes per instruction; 8 chains of two
+// lanes, 2 unrolled rounds): the FP32 peak seen by code that issues the packed form.
+__device__ __forceinline__ unsigned long long pack2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float sum2(unsigned long long r) {
+  float a, b;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+  return a + b;
+}
+__global__ void __launch_bounds__(256) fma2_probe_kernel(long long iters, float* out) {
+  unsigned long long a[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) a[i] = pack2(threadIdx.x * 1e-7f + i * 1e-7f, threadIdx.x * 1e-7f + i * 2e-7f);
+  const unsigned long long m = pack2(0.999999f, 0.999999f), c = pack2(1e-7f, 1e-7f);
+  for (long long it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int i = 0; i < 8; ++i) asm("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(a[i]) : "l"(m), "l"(c));
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += sum2(a[i]);
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 // The hot path's own division and square root (p2r::fdiv, p2r::fsqrt) over caller arrays,
 // so their error against the correctly rounded results can be measured.
 __global__ void math_check_kernel(long long n, const float* __restrict__ a, const float* __restrict__ b,
@@ -40,6 +69,15 @@ __global__ void math_check_kernel(long long n, const float* __restrict__ a, cons
 }
 
 }  // namespace
+
+extern "C" int p2r_fp32x2_fma_probe(int64_t iters, int32_t blocks, int32_t threads, float* out, void* stream) {
+  if (!out || iters < 1 || blocks < 1 || threads < 32 || threads > 256 || threads % 32)
+    return p2r_set_error(P2R_ERR_INVALID, "p2r_fp32x2_fma_probe: bad arguments");
+  fma2_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_fp32x2_fma_probe: %s", cudaGetErrorString(e));
+  return p2r_clear_error();
+}
 
 extern "C" int32_t p2r_math_variant(void) {
 #if defined(P2R_FAST_MATH)

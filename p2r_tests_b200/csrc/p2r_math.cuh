@@ -6,11 +6,18 @@
 //                    (J*C)*J^T TBB:343-373)
 //   KalmanUpdate     TBB:433-642
 // The reference evaluates these per Matriplex block with one SIMD loop per stage and
-// materialises the 6x6 Jacobian and J*C in memory. Here one thread owns one track: the
-// 6 parameters and 21 covariance elements stay in registers across layers, the Jacobian
-// is a set of 17 scalars (its unit rows 3 and 5 and its structural zeros are never
-// formed), and J*C and (J*C)*J^T are expanded at compile time over the non-zero terms,
-// in the reference's summation order.
+// materialises the 6x6 Jacobian, J*C and K*H*C in memory. Here one thread owns one track: the
+// 6 parameters and 21 covariance elements stay in registers across layers, the Jacobian is a
+// set of 17 scalars (its unit rows 3 and 5 and its structural zeros are never formed), and
+// J*C, (J*C)*J^T and C - K*(H*C) are expanded at compile time over the non-zero terms.
+//
+// Every multiply, add and fused multiply-add is written out (fmul / fadd / fsub / ffma, all
+// round-to-nearest, never re-associated or contracted by the compiler), so every kernel that
+// uses these functions (fused, per-layer, persistent queue, any launch shape) produces
+// bit-identical results. Where the reference's expression has a common factor that does not
+// change along the helix iterations (ipt/k, k*pt, k*pt/sin(theta)) it is formed once; that
+// and the fused forms change results only at the rounding level, checked against the
+// reference by the parity tests.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -19,7 +26,13 @@ namespace p2r {
 // packed lower-triangle index of a symmetric 6x6 (TBB:46-54)
 __host__ __device__ constexpr int S6(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
 
-// Division and square root, three builds:
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }  // a*b + c
+
+// ---------------------------------------------------------------- division and square root
+// Three builds:
 //  default            the hardware approximations (rcp.approx, rsqrt.approx) refined by one
 //                     Newton-Raphson step each (the textbook iteration, e.g. Markstein,
 //                     IBM J. Res. Dev. 34(1), 1990): y <- y + y (1 - b y) for 1/b, a/b = a y;
@@ -51,21 +64,30 @@ __device__ __forceinline__ float fsqrt(float x) {
 #define P2R_REFINED_MATH 1
 __device__ __forceinline__ float frcp(float b) {
   const float y = rcp_approx(b);
-  return fmaf(y, fmaf(-b, y, 1.f), y);
+  return ffma(y, ffma(-b, y, 1.f), y);
 }
-__device__ __forceinline__ float fdiv(float a, float b) { return a * frcp(b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return fmul(a, frcp(b)); }
 __device__ __forceinline__ float fsqrt(float x) {
   if (!(x > 0.f)) return sqrtf(x);
   const float r = rsqrt_approx(x);
-  const float s = x * r;
-  return fmaf(0.5f * r, fmaf(-s, s, x), s);
+  const float s = fmul(x, r);
+  return ffma(fmul(0.5f, r), ffma(-s, s, x), s);
 }
 #else
-__device__ __forceinline__ float fdiv(float a, float b) { return a / b; }
-__device__ __forceinline__ float fsqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float fsqrt(float x) { return __fsqrt_rn(x); }
 #endif
 
-__device__ __forceinline__ float hipo(float x, float y) { return fsqrt(x * x + y * y); }
+// sqrt(x^2 + y^2)
+__device__ __forceinline__ float hipo(float x, float y) { return fsqrt(ffma(x, x, fmul(y, y))); }
+
+// 1 / (e0 e2 - e1^2) with the determinant and its reciprocal in double, rounded once to float
+// (TBB:457-459). The float products are exact in double, so only the difference and the
+// reciprocal round.
+__device__ __forceinline__ float det_recip_fp64(float e0, float e1, float e2) {
+  const double det = __dsub_rn(__dmul_rn((double)e0, (double)e2), __dmul_rn((double)e1, (double)e1));
+  return (float)__drcp_rn(det);
+}
 
 // 4th-order cos / 3rd-order sin for the small per-step turning angles (TBB:644-652).
 // omc = 1 - c, evaluated as x^2/2 - x^4/24: the same polynomial without forming 1 - (1 - ...)
@@ -73,12 +95,13 @@ __device__ __forceinline__ float hipo(float x, float y) { return fsqrt(x * x + y
 // reference's -ffast-math build simplifies 1 - cosa to this form as well; evaluated as
 // written, the chained filter loses about a factor 2.5 in accuracy on 1/pT).
 __device__ __forceinline__ void sincos4(float x, float& s, float& c, float& omc) {
-  const float x2 = x * x;
-  omc = 0.5f * x2 - 0.04166667f * x2 * x2;
-  c = 1.f - omc;
-  s = x - 0.16666667f * x * x2;
+  const float x2 = fmul(x, x);
+  omc = ffma(fmul(-0.04166667f, x2), x2, fmul(0.5f, x2));
+  c = fsub(1.f, omc);
+  s = ffma(fmul(-0.16666667f, x), x2, x);
 }
 
+// ---------------------------------------------------------------- propagateToR
 // Propagates (ip, ic) to the cylinder of radius r. k = q*kfact, kinv = 1/k.
 // op/oc may be the same arrays as ip/ic: every input is read before any output is written.
 __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float (&ic)[21], float k, float kinv,
@@ -87,75 +110,96 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
   const float iptin = ip[3], phiin = ip[4], thetain = ip[5];
   float r0 = hipo(xin, yin);
   const float pt = fdiv(1.f, iptin);
+  const float ik = fmul(iptin, kinv);  // turning angle per unit of path length
+  const float kpt = fmul(k, pt);
 
-  float D = 0.f, cosa = 0.f, sina = 0.f, omc = 0.f;
   float sinP, cosP;
   sincosf(phiin, &sinP, &cosP);  // phi can be large: no approximation (TBB:688-689)
-  float pxin = cosP * pt;
-  float pyin = sinP * pt;
+  float pxin = fmul(cosP, pt);
+  float pyin = fmul(sinP, pt);
   float dDdx = r0 > 0.f ? -fdiv(xin, r0) : 0.f;
   float dDdy = r0 > 0.f ? -fdiv(yin, r0) : 0.f;
-  float dDdipt = 0.f, dDdphi = 0.f;
+  float D = 0.f, dDdipt = 0.f, dDdphi = 0.f;
+  float sina, cosa, omc;
   float xo = xin, yo = yin;
 
 #pragma unroll
   for (int i = 0; i < 5; ++i) {  // 5 fixed iterations (TBB:655, TBB:701)
     r0 = hipo(xo, yo);
-    const float id = r - r0;
-    D += id;
-    sincos4(id * iptin * kinv, sina, cosa, omc);
-    if (i + 1 != 5) {
-      // path derivatives, only once the step is below 1 um (TBB:714)
-      const float oor0 = (r0 > 0.f && fabsf(r - r0) < 0.0001f) ? fdiv(1.f, r0) : 0.f;
-      const float dadipt = id * kinv;
-      const float dadx = -xo * iptin * kinv * oor0;
-      const float dady = -yo * iptin * kinv * oor0;
-      const float pxca = pxin * cosa;
-      const float pxsa = pxin * sina;
-      const float pyca = pyin * cosa;
-      const float pysa = pyin * sina;
-      float tmp = k * dadx;
-      dDdx -= (xo * (1.f + tmp * (pxca - pysa)) + yo * tmp * (pyca + pxsa)) * oor0;
-      tmp = k * dady;
-      dDdy -= (xo * tmp * (pxca - pysa) + yo * (1.f + tmp * (pyca + pxsa))) * oor0;
-      tmp = dadipt * iptin;
-      dDdipt -= k * (xo * (pxca * tmp - pysa * tmp - pyca - pxsa + pyin) +
-                     yo * (pyca * tmp + pxsa * tmp - pysa + pxca - pxin)) * pt * oor0;
-      dDdphi += k * (xo * (pysa - pxin + pxca) - yo * (pxsa - pyin + pyca)) * oor0;
+    const float id = fsub(r, r0);
+    D = fadd(D, id);
+    sincos4(fmul(id, ik), sina, cosa, omc);
+    // Path derivatives, only once the step is below 1 um (TBB:714). The reference scales every
+    // derivative increment by oor0 = 0 until then; adding a finite x * 0 leaves the sums
+    // unchanged, so those increments are skipped.
+    if (i + 1 != 5 && r0 > 0.f && fabsf(id) < 0.0001f) {
+      const float noor0 = -fdiv(1.f, r0);  // -1/r0
+      const float kn = fmul(iptin, noor0);
+      const float tx = fmul(xo, kn), ty = fmul(yo, kn);  // k*dadx, k*dady of TBB:716-717
+      const float pxca = fmul(pxin, cosa), pxsa = fmul(pxin, sina);
+      const float pyca = fmul(pyin, cosa), pysa = fmul(pyin, sina);
+      const float a1 = fsub(pxca, pysa);
+      const float a2 = fadd(pyca, pxsa);
+      // dDdx -= (xo*(1 + tx*a1) + yo*tx*a2) * oor0
+      dDdx = ffma(ffma(xo, ffma(tx, a1, 1.f), fmul(fmul(yo, tx), a2)), noor0, dDdx);
+      // dDdy -= (xo*ty*a1 + yo*(1 + ty*a2)) * oor0
+      dDdy = ffma(ffma(yo, ffma(ty, a2, 1.f), fmul(fmul(xo, ty), a1)), noor0, dDdy);
+      // dDdipt -= k*(xo*(pxca*t - pysa*t - pyca - pxsa + pyin)
+      //             + yo*(pyca*t + pxsa*t - pysa + pxca - pxin)) * pt * oor0,  t = dadipt*ipt
+      const float t = fmul(id, ik);
+      const float e1 = ffma(a1, t, fsub(pyin, a2));
+      const float e2 = ffma(a2, t, fsub(a1, pxin));
+      dDdipt = ffma(ffma(xo, e1, fmul(yo, e2)), fmul(kpt, noor0), dDdipt);
+      // dDdphi += k*(xo*(pysa - pxin + pxca) - yo*(pxsa - pyin + pyca)) * oor0
+      const float f1 = fadd(fsub(pysa, pxin), pxca);
+      const float nf2 = fsub(fsub(pyin, pxsa), pyca);
+      dDdphi = ffma(ffma(yo, nf2, fmul(xo, f1)), fmul(-k, noor0), dDdphi);
     }
-    xo = xo + k * (pxin * sina - pyin * omc);
-    yo = yo + k * (pyin * sina + pxin * omc);
+    xo = ffma(k, ffma(pxin, sina, fmul(-pyin, omc)), xo);  // xo + k*(pxin*sina - pyin*omc)
+    yo = ffma(k, ffma(pyin, sina, fmul(pxin, omc)), yo);   // yo + k*(pyin*sina + pxin*omc)
     const float pxold = pxin;
-    pxin = pxin * cosa - pyin * sina;
-    pyin = pyin * cosa + pxold * sina;
+    pxin = ffma(pxin, cosa, fmul(-pyin, sina));
+    pyin = ffma(pxold, sina, fmul(pyin, cosa));
   }
 
-  const float alpha = D * iptin * kinv;
-  const float dadx = dDdx * iptin * kinv;
-  const float dady = dDdy * iptin * kinv;
-  const float dadipt = (iptin * dDdipt + D) * kinv;
-  const float dadphi = dDdphi * iptin * kinv;
+  const float alpha = fmul(D, ik);
+  const float dadx = fmul(dDdx, ik);
+  const float dady = fmul(dDdy, ik);
+  const float dadipt = fmul(ffma(iptin, dDdipt, D), kinv);
+  const float dadphi = fmul(dDdphi, ik);
   sincos4(alpha, sina, cosa, omc);
 
-  // non-trivial Jacobian entries (TBB:753-807); J22 = J33 = J55 = 1, the rest of rows
-  // 3 and 5 and J02 J05 J12 J15 J42 J45 are 0.
-  const float J00 = 1.f + k * dadx * (cosP * cosa - sinP * sina) * pt;
-  const float J01 = k * dady * (cosP * cosa - sinP * sina) * pt;
-  const float J03 = k * (cosP * (iptin * dadipt * cosa - sina) + sinP * (omc - iptin * dadipt * sina)) * pt * pt;
-  const float J04 = k * (cosP * dadphi * cosa - sinP * dadphi * sina - sinP * sina + cosP * cosa - cosP) * pt;
-  const float J10 = k * dadx * (sinP * cosa + cosP * sina) * pt;
-  const float J11 = 1.f + k * dady * (sinP * cosa + cosP * sina) * pt;
-  const float J13 = k * (sinP * (iptin * dadipt * cosa - sina) + cosP * (iptin * dadipt * sina - omc)) * pt * pt;
-  const float J14 = k * (sinP * dadphi * cosa + cosP * dadphi * sina + sinP * cosa + cosP * sina - sinP) * pt;
+  // Non-trivial Jacobian entries (TBB:753-807); J22 = J33 = J55 = 1, the rest of rows
+  // 3 and 5 and J02 J05 J12 J15 J42 J45 are 0. cP*ca - cP and sP*ca - sP are formed as
+  // -cP*omc and -sP*omc (the same polynomial, without the cancellation).
+  const float cc = ffma(cosP, cosa, fmul(-sinP, sina));  // cos(phi + alpha)
+  const float sc = ffma(sinP, cosa, fmul(cosP, sina));   // sin(phi + alpha)
+  const float kxp = fmul(kpt, dadx), kyp = fmul(kpt, dady);
+  const float J00 = ffma(kxp, cc, 1.f);  // 1 + k*dadx*cc*pt
+  const float J01 = fmul(kyp, cc);
+  const float J10 = fmul(kxp, sc);
+  const float J11 = ffma(kyp, sc, 1.f);
+  const float ia = fmul(iptin, dadipt);
+  const float u1 = ffma(ia, cosa, -sina);  // ipt*dadipt*cosa - sina
+  const float u2 = ffma(-ia, sina, omc);   // omc - ipt*dadipt*sina
+  const float kpt2 = fmul(kpt, pt);
+  const float J03 = fmul(ffma(cosP, u1, fmul(sinP, u2)), kpt2);   // k*(cP*u1 + sP*u2)*pt^2
+  const float J13 = fmul(ffma(sinP, u1, fmul(-cosP, u2)), kpt2);  // k*(sP*u1 - cP*u2)*pt^2
+  // k*(cP*dadphi*ca - sP*dadphi*sa - sP*sa + cP*ca - cP)*pt
+  const float J04 = fmul(ffma(dadphi, cc, -ffma(sinP, sina, fmul(cosP, omc))), kpt);
+  // k*(sP*dadphi*ca + cP*dadphi*sa + sP*ca + cP*sa - sP)*pt
+  const float J14 = fmul(ffma(dadphi, sc, ffma(cosP, sina, fmul(-sinP, omc))), kpt);
   float sinT, cosT;
   sincosf(thetain, &sinT, &cosT);  // theta can be large: no approximation (TBB:767-769)
   const float isinT = fdiv(1.f, sinT);
-  const float J20 = k * cosT * dadx * pt * isinT;
-  const float J21 = k * cosT * dady * pt * isinT;
-  const float J23 = k * cosT * (iptin * dadipt - alpha) * pt * pt * isinT;
-  const float J24 = k * dadphi * cosT * pt * isinT;
-  const float J25 = -k * alpha * pt * isinT * isinT;
-  const float J40 = dadx, J41 = dady, J43 = dadipt, J44 = 1.f + dadphi;
+  const float kpi = fmul(kpt, isinT);  // k*pt/sinT
+  const float kpc = fmul(kpi, cosT);   // k*pt*cosT/sinT
+  const float J20 = fmul(dadx, kpc);
+  const float J21 = fmul(dady, kpc);
+  const float J23 = fmul(fmul(fsub(ia, alpha), kpc), pt);
+  const float J24 = fmul(dadphi, kpc);
+  const float J25 = fmul(fmul(-alpha, kpi), isinT);  // -k*alpha*pt/sinT^2
+  const float J40 = dadx, J41 = dady, J43 = dadipt, J44 = fadd(1.f, dadphi);
 
   // T = J*C (TBB:296-341): rows 3 and 5 of T are rows 3 and 5 of C.
   float T0[6], T1[6], T2[6], T4[6];
@@ -163,10 +207,10 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
   for (int j = 0; j < 6; ++j) {
     const float c0 = ic[S6(0, j)], c1 = ic[S6(1, j)], c2 = ic[S6(2, j)];
     const float c3 = ic[S6(3, j)], c4 = ic[S6(4, j)], c5 = ic[S6(5, j)];
-    T0[j] = J00 * c0 + J01 * c1 + J03 * c3 + J04 * c4;
-    T1[j] = J10 * c0 + J11 * c1 + J13 * c3 + J14 * c4;
-    T2[j] = J20 * c0 + J21 * c1 + c2 + J23 * c3 + J24 * c4 + J25 * c5;
-    T4[j] = J40 * c0 + J41 * c1 + J43 * c3 + J44 * c4;
+    T0[j] = ffma(J04, c4, ffma(J03, c3, ffma(J01, c1, fmul(J00, c0))));
+    T1[j] = ffma(J14, c4, ffma(J13, c3, ffma(J11, c1, fmul(J10, c0))));
+    T2[j] = ffma(J25, c5, ffma(J24, c4, ffma(J23, c3, fadd(ffma(J21, c1, fmul(J20, c0)), c2))));
+    T4[j] = ffma(J44, c4, ffma(J43, c3, ffma(J41, c1, fmul(J40, c0))));
   }
   float T3[6], T5[6];
 #pragma unroll
@@ -177,14 +221,16 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
 
   // C' = T*J^T, lower triangle (TBB:343-373).
   float nc[21];
-#define P2R_ROW(i, Ti)                                                                        \
-  {                                                                                         \
-    nc[S6(i, 0)] = Ti[0] * J00 + Ti[1] * J01 + Ti[3] * J03 + Ti[4] * J04;                   \
-    if (i >= 1) nc[S6(i, 1)] = Ti[0] * J10 + Ti[1] * J11 + Ti[3] * J13 + Ti[4] * J14;       \
-    if (i >= 2) nc[S6(i, 2)] = Ti[0] * J20 + Ti[1] * J21 + Ti[2] + Ti[3] * J23 + Ti[4] * J24 + Ti[5] * J25; \
-    if (i >= 3) nc[S6(i, 3)] = Ti[3];                                                       \
-    if (i >= 4) nc[S6(i, 4)] = Ti[0] * J40 + Ti[1] * J41 + Ti[3] * J43 + Ti[4] * J44;       \
-    if (i >= 5) nc[S6(i, 5)] = Ti[5];                                                       \
+#define P2R_ROW(i, Ti)                                                                                           \
+  {                                                                                                              \
+    nc[S6(i, 0)] = ffma(Ti[4], J04, ffma(Ti[3], J03, ffma(Ti[1], J01, fmul(Ti[0], J00))));                        \
+    if (i >= 1) nc[S6(i, 1)] = ffma(Ti[4], J14, ffma(Ti[3], J13, ffma(Ti[1], J11, fmul(Ti[0], J10))));            \
+    if (i >= 2)                                                                                                  \
+      nc[S6(i, 2)] =                                                                                             \
+          ffma(Ti[5], J25, ffma(Ti[4], J24, ffma(Ti[3], J23, fadd(ffma(Ti[1], J21, fmul(Ti[0], J20)), Ti[2])))); \
+    if (i >= 3) nc[S6(i, 3)] = Ti[3];                                                                            \
+    if (i >= 4) nc[S6(i, 4)] = ffma(Ti[4], J44, ffma(Ti[3], J43, ffma(Ti[1], J41, fmul(Ti[0], J40))));            \
+    if (i >= 5) nc[S6(i, 5)] = Ti[5];                                                                            \
   }
   P2R_ROW(0, T0)
   P2R_ROW(1, T1)
@@ -196,73 +242,66 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
 
   op[0] = xo;
   op[1] = yo;
-  op[2] = zin + k * alpha * cosT * pt * isinT;
+  op[2] = ffma(alpha, kpc, zin);  // z + k*alpha*cosT*pt/sinT
   op[3] = iptin;
-  op[4] = phiin + alpha;
+  op[4] = fadd(phiin, alpha);
   op[5] = thetain;
 #pragma unroll
   for (int i = 0; i < 21; ++i) oc[i] = nc[i];
 }
 
+// ---------------------------------------------------------------- KalmanUpdate
 // Kalman update of (p, c) with a hit at hp (covariance hc), in place (TBB:433-642).
 // rhit = hipo(hp[0], hp[1]). Returns the update's chi2 = res^T inv(R) res when kChi2.
-// kFp64Det: the 2x2 determinant in double, as TBB:457-458 takes it.
+// kFp64Det: the 2x2 determinant and its reciprocal in double, as TBB:457-458 takes them.
+// H = [[rotT00, rotT01, 0, 0, 0, 0], [0, 0, 1, 0, 0, 0]] projects onto the hit's (r-phi, z)
+// plane; H*C is formed once (row 0: u, row 1: row 2 of C) and serves both the gain
+// K = C*H^T*inv(R) and the update C - K*(H*C).
 template <bool kFp64Det, bool kChi2>
 __device__ __forceinline__ float kalman_update(float (&p)[6], float (&c)[21], const float (&hp)[3],
                                                const float (&hc)[6], float rhit) {
-#if defined(P2R_FAST_MATH) || defined(P2R_REFINED_MATH)
+  // rotT00 = -(hp1 + p1)/(2 rhit), rotT01 = (hp0 + p0)/(2 rhit)
   const float inv2r = fdiv(0.5f, rhit);
-  const float rotT00 = -(hp[1] + p[1]) * inv2r;
-  const float rotT01 = (hp[0] + p[0]) * inv2r;
-#else
-  const float rotT00 = -(hp[1] + p[1]) / (2.f * rhit);
-  const float rotT01 = (hp[0] + p[0]) / (2.f * rhit);
-#endif
+  const float rotT00 = fmul(fadd(hp[1], p[1]), -inv2r);
+  const float rotT01 = fmul(fadd(hp[0], p[0]), inv2r);
 
-  const float e0 = (rotT00 * (c[0] + hc[0]) + rotT01 * (c[1] + hc[1])) * rotT00 +
-                   (rotT00 * (c[1] + hc[1]) + rotT01 * (c[2] + hc[2])) * rotT01;
-  const float e1 = (c[3] + hc[3]) * rotT00 + (c[4] + hc[4]) * rotT01;
-  const float e2 = c[5] + hc[5];
-  float s;
-  if (kFp64Det) {
-    // determinant and reciprocal in FP64, rounded once to float, as TBB:457-459 does.
-    // Kept exact in every build: the chained filter's accuracy follows the precision of s
-    // closely (an extra 0.5 ulp of random error in s alone raises the 99th-percentile
-    // covariance error by ~40 %, 2 ulp by ~4x; the other divisions and square roots are
-    // insensitive at 2 ulp).
-    const double det = (double)e0 * e2 - (double)e1 * e1;
-    s = (float)(1.0 / det);
-  } else {
-    s = fdiv(1.f, e0 * e2 - e1 * e1);
+  const float s0 = fadd(c[0], hc[0]), s1 = fadd(c[1], hc[1]), s2 = fadd(c[2], hc[2]);
+  const float e0 = ffma(ffma(rotT01, s2, fmul(rotT00, s1)), rotT01, fmul(ffma(rotT01, s1, fmul(rotT00, s0)), rotT00));
+  const float e1 = ffma(fadd(c[4], hc[4]), rotT01, fmul(fadd(c[3], hc[3]), rotT00));
+  const float e2 = fadd(c[5], hc[5]);
+  // The determinant is kept in double in every build: the chained filter's accuracy follows
+  // the precision of s closely (an extra 0.5 ulp of random error in s alone raises the
+  // 99th-percentile covariance error by ~40 %, 2 ulp by ~4x; the other divisions and square
+  // roots are insensitive at 2 ulp).
+  const float s = kFp64Det ? det_recip_fp64(e0, e1, e2) : fdiv(1.f, ffma(e0, e2, fmul(-e1, e1)));
+  const float i0 = fmul(s, e2);
+  const float i1 = fmul(-e1, s);
+  const float i2 = fmul(s, e0);
+
+  float u[6], v[6];  // rows of H*C
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    u[j] = ffma(rotT01, c[S6(1, j)], fmul(rotT00, c[S6(0, j)]));
+    v[j] = c[S6(2, j)];
   }
-  const float i0 = s * e2;
-  const float i1 = e1 * -s;
-  const float i2 = s * e0;
-
-  // gain rows m: K = C H^T inv(R), H = [[rotT00, rotT01, 0...], [0, 0, 1, 0...]]
   float K0[6], K1[6];
 #pragma unroll
   for (int m = 0; m < 6; ++m) {
-    const float cm0 = c[S6(m, 0)], cm1 = c[S6(m, 1)], cm2 = c[S6(m, 2)];
-    K0[m] = cm0 * (rotT00 * i0) + cm1 * (rotT01 * i0) + cm2 * i1;
-    K1[m] = cm0 * (rotT00 * i1) + cm1 * (rotT01 * i1) + cm2 * i2;
+    K0[m] = ffma(v[m], i1, fmul(u[m], i0));
+    K1[m] = ffma(v[m], i2, fmul(u[m], i1));
   }
-  const float res0 = rotT00 * (hp[0] - p[0]) + rotT01 * (hp[1] - p[1]);
-  const float res1 = hp[2] - p[2];
+  const float res0 = ffma(rotT01, fsub(hp[1], p[1]), fmul(rotT00, fsub(hp[0], p[0])));
+  const float res1 = fsub(hp[2], p[2]);
   float chi2 = 0.f;
-  if (kChi2) chi2 = i0 * res0 * res0 + 2.f * i1 * res0 * res1 + i2 * res1 * res1;
+  if (kChi2) chi2 = ffma(fmul(i2, res1), res1, ffma(fmul(fmul(2.f, i1), res0), res1, fmul(fmul(i0, res0), res0)));
 #pragma unroll
-  for (int m = 0; m < 6; ++m) p[m] = p[m] + K0[m] * res0 + K1[m] * res1;
+  for (int m = 0; m < 6; ++m) p[m] = ffma(K1[m], res1, ffma(K0[m], res0, p[m]));
 
-  // C' = C - K H C, lower triangle
-  float nc[21];
+  // C' = C - K*(H*C), lower triangle (u and v hold the pre-update rows)
 #pragma unroll
   for (int i = 0; i < 6; ++i)
 #pragma unroll
-    for (int j = 0; j <= i; ++j)
-      nc[S6(i, j)] = c[S6(i, j)] - (K0[i] * rotT00 * c[S6(0, j)] + K0[i] * rotT01 * c[S6(1, j)] + K1[i] * c[S6(2, j)]);
-#pragma unroll
-  for (int i = 0; i < 21; ++i) c[i] = nc[i];
+    for (int j = 0; j <= i; ++j) c[S6(i, j)] = ffma(-K1[i], v[j], ffma(-K0[i], u[j], c[S6(i, j)]));
   return chi2;
 }
 

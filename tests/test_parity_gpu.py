@@ -223,7 +223,8 @@ def test_staged_equals_plain_loads(p2r, torch, bs):
     a = gpu_forward(p2r, torch, cfg, trk, hit)
     cfg.flags = p2r.FLAG_NO_STAGING
     b = gpu_forward(p2r, torch, cfg, trk, hit)
-    parity.assert_same_arithmetic(a, b, bs, "staged vs plain loads")
+    # every operation is explicit (no compiler contraction): the variants are bit-identical
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), "staged vs plain loads"
 
 
 @pytest.mark.parametrize("threads,stages", [(32, 2), (64, 4), (96, 4), (128, 2)])
