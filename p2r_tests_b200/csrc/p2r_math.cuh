@@ -67,9 +67,10 @@ __device__ __forceinline__ float frcp(float b) {
   return ffma(y, ffma(-b, y, 1.f), y);
 }
 __device__ __forceinline__ float fdiv(float a, float b) { return fmul(a, frcp(b)); }
+// For x >= 0 (the path takes square roots of sums of squares only): x = 0 is lifted to the
+// smallest normal float for the reciprocal square root, so sqrt(+-0) = +-0 without a branch.
 __device__ __forceinline__ float fsqrt(float x) {
-  if (!(x > 0.f)) return sqrtf(x);
-  const float r = rsqrt_approx(x);
+  const float r = rsqrt_approx(fmaxf(x, 1.17549435e-38f));
   const float s = fmul(x, r);
   return ffma(fmul(0.5f, r), ffma(-s, s, x), s);
 }
@@ -89,17 +90,18 @@ __device__ __forceinline__ float det_recip_fp64(float e0, float e1, float e2) {
   return (float)__drcp_rn(det);
 }
 
-// 4th-order cos / 3rd-order sin for the small per-step turning angles (TBB:644-652).
-// omc = 1 - c, evaluated as x^2/2 - x^4/24: the same polynomial without forming 1 - (1 - ...)
-// in float, which cancels for the sub-milliradian angles of the later helix iterations (the
+// 4th-order cos / 3rd-order sin for the small per-step turning angles (TBB:644-652), as
+// s and omc = 1 - cos = x^2/2 - x^4/24. Products with cos are formed as v - v*omc: the same
+// polynomial without rounding 1 - omc first, and without forming 1 - (1 - ...) in float,
+// which cancels for the sub-milliradian angles of the later helix iterations (the
 // reference's -ffast-math build simplifies 1 - cosa to this form as well; evaluated as
 // written, the chained filter loses about a factor 2.5 in accuracy on 1/pT).
-__device__ __forceinline__ void sincos4(float x, float& s, float& c, float& omc) {
+__device__ __forceinline__ void sincos4(float x, float& s, float& omc) {
   const float x2 = fmul(x, x);
   omc = ffma(fmul(-0.04166667f, x2), x2, fmul(0.5f, x2));
-  c = fsub(1.f, omc);
   s = ffma(fmul(-0.16666667f, x), x2, x);
 }
+__device__ __forceinline__ float mulcos(float v, float omc) { return ffma(-v, omc, v); }  // v*cos
 
 // ---------------------------------------------------------------- propagateToR
 // Propagates (ip, ic) to the cylinder of radius r. k = q*kfact, kinv = 1/k.
@@ -120,7 +122,7 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
   float dDdx = r0 > 0.f ? -fdiv(xin, r0) : 0.f;
   float dDdy = r0 > 0.f ? -fdiv(yin, r0) : 0.f;
   float D = 0.f, dDdipt = 0.f, dDdphi = 0.f;
-  float sina, cosa, omc;
+  float sina, omc;
   float xo = xin, yo = yin;
 
 #pragma unroll
@@ -128,7 +130,7 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
     r0 = hipo(xo, yo);
     const float id = fsub(r, r0);
     D = fadd(D, id);
-    sincos4(fmul(id, ik), sina, cosa, omc);
+    sincos4(fmul(id, ik), sina, omc);
     // Path derivatives, only once the step is below 1 um (TBB:714). The reference scales every
     // derivative increment by oor0 = 0 until then; adding a finite x * 0 leaves the sums
     // unchanged, so those increments are skipped.
@@ -136,8 +138,8 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
       const float noor0 = -fdiv(1.f, r0);  // -1/r0
       const float kn = fmul(iptin, noor0);
       const float tx = fmul(xo, kn), ty = fmul(yo, kn);  // k*dadx, k*dady of TBB:716-717
-      const float pxca = fmul(pxin, cosa), pxsa = fmul(pxin, sina);
-      const float pyca = fmul(pyin, cosa), pysa = fmul(pyin, sina);
+      const float pxca = mulcos(pxin, omc), pxsa = fmul(pxin, sina);
+      const float pyca = mulcos(pyin, omc), pysa = fmul(pyin, sina);
       const float a1 = fsub(pxca, pysa);
       const float a2 = fadd(pyca, pxsa);
       // dDdx -= (xo*(1 + tx*a1) + yo*tx*a2) * oor0
@@ -158,8 +160,8 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
     xo = ffma(k, ffma(pxin, sina, fmul(-pyin, omc)), xo);  // xo + k*(pxin*sina - pyin*omc)
     yo = ffma(k, ffma(pyin, sina, fmul(pxin, omc)), yo);   // yo + k*(pyin*sina + pxin*omc)
     const float pxold = pxin;
-    pxin = ffma(pxin, cosa, fmul(-pyin, sina));
-    pyin = ffma(pxold, sina, fmul(pyin, cosa));
+    pxin = ffma(-pyin, sina, mulcos(pxin, omc));  // pxin*cosa - pyin*sina
+    pyin = ffma(pxold, sina, mulcos(pyin, omc));  // pyin*cosa + pxin*sina
   }
 
   const float alpha = fmul(D, ik);
@@ -167,20 +169,20 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
   const float dady = fmul(dDdy, ik);
   const float dadipt = fmul(ffma(iptin, dDdipt, D), kinv);
   const float dadphi = fmul(dDdphi, ik);
-  sincos4(alpha, sina, cosa, omc);
+  sincos4(alpha, sina, omc);
 
   // Non-trivial Jacobian entries (TBB:753-807); J22 = J33 = J55 = 1, the rest of rows
   // 3 and 5 and J02 J05 J12 J15 J42 J45 are 0. cP*ca - cP and sP*ca - sP are formed as
   // -cP*omc and -sP*omc (the same polynomial, without the cancellation).
-  const float cc = ffma(cosP, cosa, fmul(-sinP, sina));  // cos(phi + alpha)
-  const float sc = ffma(sinP, cosa, fmul(cosP, sina));   // sin(phi + alpha)
+  const float cc = ffma(-sinP, sina, mulcos(cosP, omc));  // cos(phi + alpha)
+  const float sc = ffma(cosP, sina, mulcos(sinP, omc));   // sin(phi + alpha)
   const float kxp = fmul(kpt, dadx), kyp = fmul(kpt, dady);
   const float J00 = ffma(kxp, cc, 1.f);  // 1 + k*dadx*cc*pt
   const float J01 = fmul(kyp, cc);
   const float J10 = fmul(kxp, sc);
   const float J11 = ffma(kyp, sc, 1.f);
   const float ia = fmul(iptin, dadipt);
-  const float u1 = ffma(ia, cosa, -sina);  // ipt*dadipt*cosa - sina
+  const float u1 = fsub(mulcos(ia, omc), sina);  // ipt*dadipt*cosa - sina
   const float u2 = ffma(-ia, sina, omc);   // omc - ipt*dadipt*sina
   const float kpt2 = fmul(kpt, pt);
   const float J03 = fmul(ffma(cosP, u1, fmul(sinP, u2)), kpt2);   // k*(cP*u1 + sP*u2)*pt^2
