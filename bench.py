@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--uneven-steps", type=int, default=10)
+    ap.add_argument("--no-calib", action="store_true", help="skip the 40-layer calibration workload")
+    ap.add_argument("--calib-steps", type=int, default=3)
+    ap.add_argument("--calib-nevts", type=int, default=100)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
     ap.add_argument("--ref-budget", type=float, default=90.0, help="reference arm: total seconds")
     return ap.parse_args()
@@ -394,6 +397,67 @@ def main():
                   "autotune_candidates": len(tq["tried"])}
         del qt, qh, qo, wl
 
+    # calibration workload: 1e5 tracks x 100 events x 40 layers (r = 4..110 cm), generated on
+    # the device, 20-40 layers per track, radius offsets of +-100 um; the forward alone
+    # (masked fused forward) and forward + adjoint with per-event chi2 gradients w.r.t. the 40
+    # offsets and Bz, captured once in a CUDA graph and replayed
+    calib = None
+    if not args.no_calib and world == 1:
+        c4 = p2r.Config(bsize=32, nlayer=40, nevts=args.calib_nevts, nb=3125, bz=BZ)
+        gp4 = p2r.gen_params(bz=BZ, seed=20240004, r_first=4.0, r_last=110.0)
+        gen0, gen1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        gen0.record(stream)
+        t4, h4 = p2r.generate_helix_device(c4, gp4, stream=stream)
+        gen1.record(stream)
+        g4 = torch.Generator(dev).manual_seed(4)
+        nl4 = torch.randint(20, 41, (c4.ntracks,), dtype=torch.int32, device=dev, generator=g4)
+        dr4 = (torch.rand(c4.nlayer, device=dev, generator=g4) * 0.02 - 0.01).contiguous()
+        upd4 = int(nl4.sum().item())
+        o4 = torch.empty_like(t4)
+        for _ in range(2):
+            p2r.forward(c4, t4, h4, o4, dr=dr4, nlay_lane=nl4, stream=stream)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.calib_steps):
+            p2r.forward(c4, t4, h4, o4, dr=dr4, nlay_lane=nl4, stream=stream)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fms = f0.elapsed_time(f1) / args.calib_steps
+        del o4
+        gc4 = torch.ones(c4.ntracks, dtype=torch.float32, device=dev)
+        out4 = {"grad_trk_in": None, "grad_hits": None}
+        p2r.forward_backward(c4, t4, h4, dr=dr4, nlay_lane=nl4, grad_chi2=gc4, per_event=True, out=out4,
+                             stream=stream)
+        torch.cuda.synchronize()
+        graph4 = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream(device=dev)  # capture needs a non-default stream; replays run on the current one
+        with torch.cuda.graph(graph4, stream=cap):
+            p2r.forward_backward(c4, t4, h4, dr=dr4, nlay_lane=nl4, grad_chi2=gc4, per_event=True, out=out4,
+                                 stream=cap)
+        graph4.replay()
+        torch.cuda.synchronize()
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(args.calib_steps):
+            graph4.replay()
+        b1.record(stream)
+        torch.cuda.synchronize()
+        bms = b0.elapsed_time(b1) / args.calib_steps
+        ev_sum = out4["grad_dr_event"].sum(0)
+        calib = {"workload": f"{c4.ntracks // c4.nevts} tracks x {c4.nevts} events x 40 layers, hits on r = 4..110 cm, "
+                             "20-40 layers per track (uniform), dr ~ U[-100, 100] um, generated on the device",
+                 "hits_bytes": h4.numel() * 4, "tracks_bytes": t4.numel() * 4, "updates": upd4,
+                 "device_generation_ms": gen0.elapsed_time(gen1),
+                 "forward": {"ms_per_step": fms, "updates_per_s": upd4 / (fms / 1e3),
+                             "api": "p2r_forward_masked (fused, per-track layer counts)"},
+                 "forward_adjoint": {"ms_per_step": bms, "ratio_vs_forward": bms / fms,
+                                     "api": "p2r_forward_backward (FP64, ckpt 5), per-event grad_dr/grad_bz, "
+                                            "replayed from one CUDA graph"},
+                 "per_event_sum_matches_total": bool(torch.allclose(ev_sum, out4["grad_dr"], rtol=1e-10, atol=0)),
+                 "steps": args.calib_steps}
+        del graph4, out4, t4, h4, nl4, gc4
+
     # end to end through the host-buffer C-ABI call: H2D + kernels + D2H every step
     h_trk = torch.from_numpy(trk.reshape(-1)).pin_memory().numpy()
     h_hit = torch.from_numpy(hit.reshape(-1)).pin_memory().numpy()
@@ -453,6 +517,7 @@ def main():
             "fwd_adjoint": adjoint,
             "bsize_sweep": sweep,
             "uneven_batch": uneven,
+            "calibration_40_layers": calib,
             "gpu_launches": args.steps,
             "clocks": clk,
             "nonfinite_tracks": nonfinite,

@@ -302,6 +302,14 @@ void p2r_gen_params_default(p2r_gen_params* gp);
 int p2r_gen_helix(const p2r_gen_params* gp, int32_t bsize, int64_t nevts, int64_t nb, int32_t nlayer,
                   const int32_t* ntrk_event, void* host_trk, void* host_hits, int32_t nthreads);
 
+/* The same generator on the device: DEVICE arrays trk_out / hits_out, ntrk_event a DEVICE
+ * pointer (nullable), stream-ordered. Same random streams and arithmetic as p2r_gen_helix;
+ * the outputs equal its outputs bit for bit except for rare 1-ulp differences where the
+ * device and host transcendental functions round differently. No reference counterpart
+ * (the reference generates its inputs on the host, TBB:243-293). */
+int p2r_gen_helix_device(const p2r_gen_params* gp, int32_t bsize, int64_t nevts, int64_t nb, int32_t nlayer,
+                         const int32_t* ntrk_event, void* trk_out, void* hits_out, void* stream);
+
 /* The reference's input recipe (prepareTracks / prepareHits, TBB:243-293 with randn
  * TBB:127-145) on HOST arrays, from a caller-supplied seed track (par[6], cov[21], q) and
  * n_input_hits hits (pos[3], cov[6] each, in layer order). Draws from glibc rand() in the

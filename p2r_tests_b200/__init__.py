@@ -7,7 +7,7 @@ in include/p2r.h); this package is the Python host side over that ABI.
 from ._lib import (FLAG_ADJ_FP32, FLAG_FP32_DET, FLAG_NO_STAGING, MODE_CHAINED, MODE_RESTART, P2RError, LIB_PATH, lib)
 from .api import (Config, KalmanUpdate, REF_BZ, count_nonfinite, forward, forward_host, fp32_fma_probe, gen_params,
                   generate_fixture,
-                  generate_helix, kfact, math_check, math_variant, propagateToR, run_layers, summary, tracks_cov, tracks_par, tracks_q)
+                  generate_helix, generate_helix_device, kfact, math_check, math_variant, propagateToR, run_layers, summary, tracks_cov, tracks_par, tracks_q)
 
 from .autograd import P2RChain, forward_backward, workspace_size
 from .uneven import Queue, lognormal_counts, plan, uneven_workload
@@ -17,6 +17,6 @@ __all__ = [
     "P2RChain", "forward_backward", "workspace_size", "Queue", "lognormal_counts", "plan", "uneven_workload",
     "Config", "KalmanUpdate", "propagateToR", "run_layers", "forward", "forward_host", "fp32_fma_probe",
     "count_nonfinite", "kfact", "math_check", "math_variant",
-    "gen_params", "generate_helix", "generate_fixture", "summary", "tracks_par", "tracks_cov", "tracks_q",
+    "gen_params", "generate_helix", "generate_helix_device", "generate_fixture", "summary", "tracks_par", "tracks_cov", "tracks_q",
     "MODE_CHAINED", "MODE_RESTART", "FLAG_ADJ_FP32", "FLAG_FP32_DET", "FLAG_NO_STAGING", "P2RError", "REF_BZ", "LIB_PATH", "lib",
 ]

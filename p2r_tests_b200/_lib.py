@@ -128,6 +128,7 @@ SIGNATURES = {
                                             _vp, _vp, _i32, _vp, ctypes.c_size_t, _vp]),
     "p2r_gen_params_default": (None, [ctypes.POINTER(CGenParams)]),
     "p2r_gen_helix": (ctypes.c_int, [ctypes.POINTER(CGenParams), _i32, _i64, _i64, _i32, _vp, _vp, _vp, _i32]),
+    "p2r_gen_helix_device": (ctypes.c_int, [ctypes.POINTER(CGenParams), _i32, _i64, _i64, _i32, _vp, _vp, _vp, _vp]),
     "p2r_gen_fixture": (ctypes.c_int, [_vp, _vp, _i32, _vp, _i32, _i32, _i64, _i64, _i32, ctypes.c_double, _vp, _vp]),
     "p2r_summary": (ctypes.c_int, [_vp, _i32, _i64, _i64, _vp, ctypes.POINTER(CSummary)]),
 }

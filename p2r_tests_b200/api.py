@@ -200,6 +200,25 @@ def generate_helix(cfg: Config, params: CGenParams | None = None, ntrk_event=Non
     return trk, hit
 
 
+def generate_helix_device(cfg: Config, params: CGenParams | None = None, ntrk_event=None, stream=None,
+                          device=None):
+    """generate_helix on the GPU: returns flat float32 device tensors (tracks, hits) in
+    Matriplex layout, the same values as the host generator (rare 1-ulp differences)."""
+    import torch
+    gp = params if params is not None else gen_params(bz=cfg.bz)
+    dev = torch.device("cuda") if device is None else torch.device(device)
+    trk = torch.empty(cfg.nblocks * TRK_WORDS * cfg.bsize, dtype=torch.float32, device=dev)
+    hit = torch.empty(cfg.nblocks * cfg.nlayer * HIT_WORDS * cfg.bsize, dtype=torch.float32, device=dev)
+    nte = None
+    if ntrk_event is not None:
+        nte = torch.as_tensor(np.asarray(ntrk_event, dtype=np.int32)).to(dev)
+        if nte.shape != (cfg.nevts,):
+            raise P2RError(_lib.P2R_ERR_INVALID, "ntrk_event needs one entry per event")
+    check(lib().p2r_gen_helix_device(ctypes.byref(gp), cfg.bsize, cfg.nevts, cfg.nb, cfg.nlayer, _ptr(nte),
+                                     _ptr(trk), _ptr(hit), _stream(stream)))
+    return trk, hit
+
+
 def generate_fixture(seed_par, seed_cov, seed_q: int, input_hits, cfg: Config, smear: float = 1e-5):
     """The reference's recipe (TBB:243-293) from a seed track and per-layer hits (pos 3, cov 6)."""
     par = np.ascontiguousarray(seed_par, np.float32)

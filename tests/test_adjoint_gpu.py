@@ -200,3 +200,47 @@ def test_adjoint_rejects_bad_requests(p2r, torch):
     cfg.mode = p2r.MODE_RESTART
     with pytest.raises(p2r.P2RError):
         p2r.forward_backward(cfg, d(trk), d(hit))
+
+
+def test_calibration_gradients_config4_shape(p2r, torch):
+    """The calibration use of the adjoint in the shape of the 40-layer workload (hits on
+    r = 4..110 cm, inputs generated on the device, 20-40 layers per track, radius offsets of
+    +-100 um): per-event chi2 gradients w.r.t. the 40 offsets and Bz, captured in a CUDA graph
+    and replayed, against the FP64 reference computed event by event."""
+    nevts, nb, nlayer = 2, 4, 40
+    cfg = p2r.Config(bsize=32, nlayer=nlayer, nevts=nevts, nb=nb, bz=3.8)
+    gp = p2r.gen_params(bz=3.8, seed=4040, r_first=4.0, r_last=110.0)
+    trk_d, hit_d = p2r.generate_helix_device(cfg, gp)
+    rng = np.random.default_rng(4)
+    nlay = rng.integers(20, nlayer + 1, cfg.ntracks).astype(np.int32)
+    dr = rng.uniform(-0.01, 0.01, nlayer).astype(np.float32)
+    d_nlay, d_dr = torch.from_numpy(nlay).cuda(), torch.from_numpy(dr).cuda()
+    g_chi2 = torch.ones(cfg.ntracks, dtype=torch.float32, device="cuda")
+    out = {"grad_trk_in": None, "grad_hits": None}
+    p2r.forward_backward(cfg, trk_d, hit_d, dr=d_dr, nlay_lane=d_nlay, grad_chi2=g_chi2, per_event=True, out=out)
+    torch.cuda.synchronize()
+    direct = {k: out[k].clone() for k in ("grad_dr_event", "grad_bz_event", "chi2")}
+    for k in ("grad_dr_event", "grad_bz_event", "chi2"):
+        out[k].zero_()
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        p2r.forward_backward(cfg, trk_d, hit_d, dr=d_dr, nlay_lane=d_nlay, grad_chi2=g_chi2, per_event=True, out=out,
+                             stream=s)
+    g.replay()
+    torch.cuda.synchronize()
+    for k in direct:  # graph replay == direct call, bit for bit (deterministic reductions)
+        assert torch.equal(direct[k], out[k]), k
+    trk, hit = trk_d.cpu().numpy(), hit_d.cpu().numpy()
+    per_ev_trk, per_ev_hit = trk.size // nevts, hit.size // nevts
+    g_trk0 = np.zeros(per_ev_trk, np.float32)
+    for e in range(nevts):
+        ce = p2r.Config(bsize=32, nlayer=nlayer, nevts=1, nb=nb, bz=3.8)
+        te = trk[e * per_ev_trk:(e + 1) * per_ev_trk]
+        he = hit[e * per_ev_hit:(e + 1) * per_ev_hit]
+        ne = nlay[e * nb * 32:(e + 1) * nb * 32]
+        ref = torch_reference(p2r, ce, te, he, dr, g_trk0, np.ones(nb * 32, np.float32), nlay=ne)
+        got_dr = out["grad_dr_event"][e].cpu().numpy()
+        assert grad_err(got_dr, ref["dr"]).max() < GRAD_RTOL, (e, grad_err(got_dr, ref["dr"]).max())
+        assert grad_err([float(out["grad_bz_event"][e])], [ref["bz"]])[0] < GRAD_RTOL
+    del g

@@ -1,0 +1,45 @@
+"""The device-side helix generator against the host generator: same random streams and
+arithmetic, so the arrays agree bit for bit except where CUDA's and the C library's
+double-precision transcendentals round differently (then by one float ulp), including
+per-event track counts (padding lanes) and several bsize / layer counts."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("bs,nevts,nb,nlayer", [(32, 3, 7, 20), (1, 2, 5, 3), (64, 2, 3, 40), (96, 1, 2, 25)])
+def test_device_generator_matches_host(bs, nevts, nb, nlayer):
+    import torch
+    import p2r_tests_b200 as p2r
+    cfg = p2r.Config(bsize=bs, nlayer=nlayer, nevts=nevts, nb=nb, bz=3.8)
+    gp = p2r.gen_params(bz=3.8, seed=1234 + bs, r_first=4.0, r_last=110.0)
+    counts = None if bs == 1 else np.array([nb * bs - 5 - e for e in range(nevts)], np.int32)
+    trk_h, hit_h = p2r.generate_helix(cfg, gp, ntrk_event=counts)
+    trk_d, hit_d = p2r.generate_helix_device(cfg, gp, ntrk_event=counts)
+    torch.cuda.synchronize()
+    for host, dev in ((trk_h.reshape(-1), trk_d.cpu().numpy()), (hit_h.reshape(-1), hit_d.cpu().numpy())):
+        a, b = host.view(np.int32).astype(np.int64), dev.view(np.int32).astype(np.int64)
+        ulps = np.abs(a - b)
+        assert ulps.max() <= 1, ulps.max()
+        assert (ulps > 0).mean() < 1e-4, (ulps > 0).mean()
+
+
+def test_device_generator_feeds_the_forward():
+    """Generated on the device, the chained forward runs and every track stays finite."""
+    import torch
+    import p2r_tests_b200 as p2r
+    cfg = p2r.Config(bsize=32, nlayer=20, nevts=4, nb=30, bz=3.8)
+    trk, hit = p2r.generate_helix_device(cfg)
+    out = torch.empty_like(trk)
+    p2r.forward(cfg, trk, hit, out)
+    assert p2r.count_nonfinite(out, cfg.nblocks, cfg.bsize) == 0
+
+
+def test_device_generator_empty_and_invalid():
+    import torch
+    import p2r_tests_b200 as p2r
+    cfg = p2r.Config(bsize=32, nlayer=20, nevts=0, nb=4, bz=3.8)
+    p2r.generate_helix_device(cfg)  # empty batch: no launch
+    with pytest.raises(p2r.P2RError):
+        p2r.generate_helix_device(p2r.Config(bsize=32, nlayer=20, nevts=1, nb=1, bz=0.0))
