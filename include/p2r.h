@@ -203,10 +203,16 @@ int p2r_graph_destroy(p2r_graph* g);
  * differences; its trk_out / chi2_out are that FP64 forward rounded to float (closer to the
  * exact result than p2r_forward's FP32 chain). cfg->flags & P2R_FLAG_ADJ_FP32 runs the same
  * kernel in FP32: several times faster, gradients accurate to ~1e-2 where chi2 enters.
- * workspace: device memory of p2r_forward_backward_workspace_size(cfg) bytes, 256-byte
- * aligned (per-warp partial sums of the shared gradients, reduced in a fixed order in
- * double, so results are deterministic). */
+ * workspace: device memory of at least p2r_forward_backward_workspace_size(cfg) bytes,
+ * 256-byte aligned (per-warp partial sums of the shared gradients, reduced in a fixed order
+ * in double, so results are deterministic). With the checkpoints held per thread, the
+ * kernel keeps them in thread-local memory; a workspace of
+ * p2r_forward_backward_workspace_size_tape(cfg, ckpt_stride) bytes also holds them, and the
+ * recomputed segment states, as a tape in device memory ([slot][27][thread], 27*(nlayer /
+ * ckpt_stride + ckpt_stride - 1) values per track), which runs the forward and the reverse
+ * as two lighter kernels. Same results either way. */
 size_t p2r_forward_backward_workspace_size(const p2r_config* cfg);
+size_t p2r_forward_backward_workspace_size_tape(const p2r_config* cfg, int32_t ckpt_stride);
 int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* hits, const float* dr,
                          const int32_t* nlay_lane, void* trk_out, float* chi2_out, const void* grad_trk_out,
                          const float* grad_chi2, void* grad_trk_in, void* grad_hits, double* grad_dr,

@@ -115,6 +115,7 @@ SIGNATURES = {
     "p2r_math_variant": (ctypes.c_int32, []),
     "p2r_math_check": (ctypes.c_int, [_i64, _vp, _vp, _vp, _vp, _vp]),
     "p2r_forward_backward_workspace_size": (ctypes.c_size_t, [_cfgp]),
+    "p2r_forward_backward_workspace_size_tape": (ctypes.c_size_t, [_cfgp, _i32]),
     "p2r_forward_backward_noalloc": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                                     _vp, _vp, _vp, _i32, _vp]),
     "p2r_queue_plan": (ctypes.c_int64, [_vp, _i64, _i32, _vp, _i64]),

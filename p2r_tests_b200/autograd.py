@@ -18,17 +18,25 @@ from ._lib import P2RError, check, lib
 from .api import Config, HIT_WORDS, TRK_WORDS, _check_shapes, _ptr, _stream
 
 
-def workspace_size(cfg: Config) -> int:
+def workspace_size(cfg: Config, ckpt_stride: int | None = None) -> int:
+    """Workspace bytes of p2r_forward_backward: the minimum (checkpoints in thread-local
+    memory) when ckpt_stride is None, else the size that also holds the checkpoint tape."""
     c = cfg.c()
-    n = lib().p2r_forward_backward_workspace_size(ctypes.byref(c))
+    if ckpt_stride is None:
+        n = lib().p2r_forward_backward_workspace_size(ctypes.byref(c))
+    else:
+        n = lib().p2r_forward_backward_workspace_size_tape(ctypes.byref(c), ckpt_stride)
     if n == 0:
         raise P2RError(_lib.P2R_ERR_INVALID, lib().p2r_last_error_string().decode())
     return int(n)
 
 
 def forward_backward(cfg: Config, trk_in, hits, dr=None, nlay_lane=None, grad_trk_out=None, grad_chi2=None,
-                     ckpt_stride: int = 5, per_event: bool = False, stream=None, out=None) -> dict:
-    """Returns trk_out, chi2, grad_trk_in, grad_hits, grad_dr, grad_bz (and *_event)."""
+                     ckpt_stride: int = 5, per_event: bool = False, stream=None, out=None, tape: bool = True) -> dict:
+    """Returns trk_out, chi2, grad_trk_in, grad_hits, grad_dr, grad_bz (and *_event).
+    tape: give the library a workspace that holds the checkpoint tape (two-kernel path);
+    False keeps the checkpoints in thread-local memory (smallest workspace). An entry of
+    `out` set to None skips that output (e.g. grad_hits for calibration-only runs)."""
     _check_shapes(cfg, trk_in, hits)
     dev = trk_in.device
     o = out if out is not None else {}
@@ -44,7 +52,7 @@ def forward_backward(cfg: Config, trk_in, hits, dr=None, nlay_lane=None, grad_tr
         o.setdefault("grad_dr_event", torch.empty(cfg.nevts, cfg.nlayer, **f64))
         o.setdefault("grad_bz_event", torch.empty(cfg.nevts, **f64))
     ws = o.get("workspace")
-    need = workspace_size(cfg)
+    need = workspace_size(cfg, ckpt_stride if tape else None)
     if ws is None or ws.numel() < need:
         ws = torch.empty(need, dtype=torch.uint8, device=dev)
         o["workspace"] = ws

@@ -214,6 +214,187 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
   }
 }
 
+// ---------------------------------------------------------------- tape path
+// The same computation as fwdbwd_kernel split in two kernels, with the checkpoints and the
+// recomputed segment states in a tape in device memory instead of thread-local arrays:
+// fwd_tape_kernel runs the forward and stores the state every CK layers; rev_tape_kernel
+// walks the segments backwards, recomputes each segment's states once into a segment
+// buffer, and reverses the layers. Layout of both: [slot][27 components][thread], so a warp's
+// 32 lanes read and write one 256-byte (double) or 128-byte (float) line per component.
+// Used when the caller's workspace holds the tape (p2r_forward_backward_workspace_size_tape).
+struct TapeParams {
+  void* tape;      // [nslots][27][nthreads] of T: the state before layers 0, CK, 2 CK, ...
+  void* segbuf;    // [CK - 1][27][nthreads] of T: the state before layers a+1 .. a+CK-1
+  long long nthreads;
+};
+
+template <class T>
+__device__ __forceinline__ void tape_store(T* base, long long nthreads, long long g, const T (&par)[6],
+                                           const T (&cov)[21]) {
+#pragma unroll
+  for (int i = 0; i < 6; ++i) base[i * nthreads + g] = par[i];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) base[(6 + i) * nthreads + g] = cov[i];
+}
+template <class T>
+__device__ __forceinline__ void tape_load(const T* base, long long nthreads, long long g, T (&par)[6], T (&cov)[21]) {
+#pragma unroll
+  for (int i = 0; i < 6; ++i) par[i] = base[i * nthreads + g];
+#pragma unroll
+  for (int i = 0; i < 21; ++i) cov[i] = base[(6 + i) * nthreads + g];
+}
+
+// Per-thread set-up shared by both tape kernels.
+template <class T>
+struct TrackCtx {
+  long long g, b;
+  int it, lane, nl, nl_warp, q;
+  bool valid;
+  T k, kinv;
+  const float* hblk;
+  __device__ TrackCtx(const AdjParams& p, T (&par)[6], T (&cov)[21]) {
+    const int bs = p.bsize;
+    lane = threadIdx.x & 31;
+    g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    b = g / bs;
+    it = (int)(g - b * bs);
+    valid = b < p.nblocks;
+    q = 1;
+    nl = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) par[i] = (i == 3 || i == 5) ? T(1) : T(0);
+#pragma unroll
+    for (int i = 0; i < 21; ++i) cov[i] = 0;
+    if (valid) {
+      const float* tb = p.trk_in + b * (long long)(28 * bs);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) par[i] = (T)tb[i * bs + it];
+#pragma unroll
+      for (int i = 0; i < 21; ++i) cov[i] = (T)tb[(6 + i) * bs + it];
+      q = __float_as_int(tb[27 * bs + it]);
+      nl = p.nlay ? min(p.nlayer, max(0, p.nlay[b * bs + it])) : p.nlayer;
+    }
+    const T kfact = (sizeof(T) == sizeof(float)) ? (T)p.kfact : (T)(100.0 / (-0.299792458 * p.bz));
+    k = (T)q * kfact;
+    kinv = T(1) / k;
+    nl_warp = nl;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nl_warp = max(nl_warp, __shfl_xor_sync(0xffffffffu, nl_warp, o));
+    hblk = p.hits + b * (long long)p.nlayer * (9 * bs);
+  }
+};
+
+template <class T, int CK>
+__global__ void __launch_bounds__(kAdjThreads) fwd_tape_kernel(AdjParams p, TapeParams tp) {
+  T par[6], cov[21];
+  const TrackCtx<T> c(p, par, cov);
+  const int bs = p.bsize;
+  T* tape = (T*)tp.tape;
+  T chi2 = 0;
+  for (int l = 0; l < c.nl; ++l) {
+    if (l % CK == 0) tape_store(tape + (long long)(l / CK) * 27 * tp.nthreads, tp.nthreads, c.g, par, cov);
+    T hp[3], hc[6];
+    load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
+    chi2 += adj::layer_fwd(par, cov, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0));
+  }
+  if (c.valid) {
+    if (p.trk_out) {
+      float* ob = p.trk_out + c.b * (long long)(28 * bs);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) ob[i * bs + c.it] = (float)par[i];
+#pragma unroll
+      for (int i = 0; i < 21; ++i) ob[(6 + i) * bs + c.it] = (float)cov[i];
+      ob[27 * bs + c.it] = __int_as_float(c.q);
+    }
+    if (p.chi2_out) p.chi2_out[c.b * bs + c.it] = (float)chi2;
+  }
+}
+
+template <class T, int CK>
+__global__ void __launch_bounds__(kAdjThreads) rev_tape_kernel(AdjParams p, TapeParams tp) {
+  T par[6], cov[21];
+  const TrackCtx<T> c(p, par, cov);
+  const int bs = p.bsize;
+  const T* tape = (const T*)tp.tape;
+  T* segbuf = (T*)tp.segbuf;
+  float* wpart = p.partials + (c.g >> 5) * (p.nlayer + 1);
+  T pb[6] = {}, cb[21] = {};
+  T chi2b = 0;
+  if (c.valid) {
+    if (p.g_trk_out) {
+      const float* gb = p.g_trk_out + c.b * (long long)(28 * bs);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) pb[i] = (T)gb[i * bs + c.it];
+#pragma unroll
+      for (int i = 0; i < 21; ++i) cb[i] = (T)gb[(6 + i) * bs + c.it];
+    }
+    if (p.g_chi2) chi2b = (T)p.g_chi2[c.b * bs + c.it];
+  }
+  T kbar = 0, kinvbar = 0;
+  const int nseg = (c.nl_warp + CK - 1) / CK;
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int a = seg * CK;
+    const int e = min(a + CK, c.nl_warp);
+    if (CK > 1 && a + 1 < min(e, c.nl)) {
+      // states before layers a+1 .. e-1, recomputed once from the checkpoint
+      T sp[6], sc[21];
+      tape_load(tape + (long long)seg * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
+      for (int l = a + 1; l < e && l < c.nl; ++l) {
+        T hp[3], hc[6];
+        load_hit_t(c.hblk + (long long)(l - 1) * (9 * bs), bs, c.it, hp, hc);
+        adj::layer_fwd(sp, sc, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l - 1] : T(0));
+        tape_store(segbuf + (long long)(l - a - 1) * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
+      }
+    }
+    for (int l = e - 1; l >= a; --l) {
+      T drb = 0;
+      if (l < c.nl) {
+        T sp[6], sc[21];
+        if (l == a)
+          tape_load(tape + (long long)seg * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
+        else
+          tape_load(segbuf + (long long)(l - a - 1) * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
+        T hp[3], hc[6], hpb[3], hcb[6];
+        load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
+        adj::layer_rev(sp, sc, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0), pb, cb, chi2b, hpb, hcb, drb, kbar,
+                       kinvbar);
+        if (p.g_hits) {
+          float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
+#pragma unroll
+          for (int i = 0; i < 3; ++i) gh[i * bs + c.it] = (float)hpb[i];
+#pragma unroll
+          for (int i = 0; i < 6; ++i) gh[(3 + i) * bs + c.it] = (float)hcb[i];
+        }
+      } else if (c.valid && p.g_hits) {
+        float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) gh[i * bs + c.it] = 0.f;
+      }
+      drb = warp_sum_t(drb);
+      if (c.lane == 0) wpart[l] = (float)drb;
+    }
+  }
+  if (c.lane == 0)
+    for (int l = c.nl_warp; l < p.nlayer; ++l) wpart[l] = 0.f;
+  if (c.valid && p.g_hits)
+    for (int l = c.nl_warp; l < p.nlayer; ++l) {
+      float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) gh[i * bs + c.it] = 0.f;
+    }
+  T bzb = c.valid ? (kbar - kinvbar * c.kinv * c.kinv) * (-c.k / (T)p.bz) : T(0);
+  bzb = warp_sum_t(bzb);
+  if (c.lane == 0) wpart[p.nlayer] = (float)bzb;
+  if (c.valid && p.g_trk_in) {
+    float* gb = p.g_trk_in + c.b * (long long)(28 * bs);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) gb[i * bs + c.it] = (float)pb[i];
+#pragma unroll
+    for (int i = 0; i < 21; ++i) gb[(6 + i) * bs + c.it] = (float)cb[i];
+    gb[27 * bs + c.it] = 0.f;
+  }
+}
+
 // Sums per-warp partials [nwarps][nout] in a fixed order, in double. Block (e, j) sums
 // warps [e*wpe, min((e+1)*wpe, nwarps)) of column j into out[e*nout + j].
 __global__ void __launch_bounds__(256) sum_partials_kernel(const float* partials, long long nwarps, int nout,
@@ -279,6 +460,46 @@ WsLayout layout_of(const p2r_config* cfg) {
   return w;
 }
 
+// Tape region after the partial sums: [nslots][27][nthreads] checkpoints, then
+// [CK - 1][27][nthreads] segment states, in the kernel's arithmetic type.
+struct TapeLayout {
+  long long nthreads;
+  size_t tape_off, seg_off, end;
+};
+
+TapeLayout tape_layout_of(const p2r_config* cfg, int ck, size_t elem) {
+  TapeLayout t;
+  const long long ntr = (long long)cfg->nevts * cfg->nb * cfg->bsize;
+  t.nthreads = (ntr + kAdjThreads - 1) / kAdjThreads * kAdjThreads;
+  const long long nslots = (cfg->nlayer + ck - 1) / ck;
+  const size_t per_slot = (size_t)27 * t.nthreads * elem;
+  t.tape_off = (layout_of(cfg).total_bytes + 255) & ~(size_t)255;
+  t.seg_off = t.tape_off + (((size_t)nslots * per_slot + 255) & ~(size_t)255);
+  t.end = t.seg_off + (size_t)(ck - 1) * per_slot;
+  return t;
+}
+
+int normal_ckpt(int ckpt_stride) { return ckpt_stride == 0 ? 5 : ckpt_stride; }
+
+template <class T, int CK>
+cudaError_t launch_tape(const AdjParams& p, const TapeParams& tp, cudaStream_t st) {
+  const unsigned grid = (unsigned)(tp.nthreads / kAdjThreads);
+  fwd_tape_kernel<T, CK><<<grid, kAdjThreads, 0, st>>>(p, tp);
+  rev_tape_kernel<T, CK><<<grid, kAdjThreads, 0, st>>>(p, tp);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_tape_ck(const AdjParams& p, const TapeParams& tp, int ck, cudaStream_t st) {
+  switch (ck) {
+    case 1: return launch_tape<T, 1>(p, tp, st);
+    case 2: return launch_tape<T, 2>(p, tp, st);
+    case 4: return launch_tape<T, 4>(p, tp, st);
+    case 10: return launch_tape<T, 10>(p, tp, st);
+    default: return launch_tape<T, 5>(p, tp, st);
+  }
+}
+
 template <class T, int CK>
 cudaError_t launch_fwdbwd(const AdjParams& p, long long ntr, cudaStream_t st) {
   const long long grid = (ntr + kAdjThreads - 1) / kAdjThreads;
@@ -304,6 +525,13 @@ extern "C" {
 size_t p2r_forward_backward_workspace_size(const p2r_config* cfg) {
   if (p2r_check_config(cfg, "p2r_forward_backward_workspace_size")) return 0;
   return layout_of(cfg).total_bytes;
+}
+
+size_t p2r_forward_backward_workspace_size_tape(const p2r_config* cfg, int32_t ckpt_stride) {
+  if (p2r_check_config(cfg, "p2r_forward_backward_workspace_size_tape")) return 0;
+  const int ck = normal_ckpt(ckpt_stride);
+  if (ck != 1 && ck != 2 && ck != 4 && ck != 5 && ck != 10) return 0;
+  return tape_layout_of(cfg, ck, (cfg->flags & P2R_FLAG_ADJ_FP32) ? sizeof(float) : sizeof(double)).end;
 }
 
 int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* hits, const float* dr,
@@ -349,10 +577,21 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   if (ckpt_stride != 0 && ckpt_stride != 1 && ckpt_stride != 2 && ckpt_stride != 4 && ckpt_stride != 5 &&
       ckpt_stride != 10)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: checkpoint stride %d (use 1, 2, 4, 5 or 10)", who, ckpt_stride);
-  if (cfg->flags & P2R_FLAG_ADJ_FP32)
-    e = launch_fwdbwd_ck<float>(p, ntr, ckpt_stride, st);
-  else
-    e = launch_fwdbwd_ck<double>(p, ntr, ckpt_stride, st);
+  const bool fp32 = (cfg->flags & P2R_FLAG_ADJ_FP32) != 0;
+  const int ck = normal_ckpt(ckpt_stride);
+  const TapeLayout tl = tape_layout_of(cfg, ck, fp32 ? sizeof(float) : sizeof(double));
+  if (workspace_bytes >= tl.end) {
+    // the workspace holds the tape: two kernels, checkpoints and segment states in memory
+    TapeParams tp;
+    tp.tape = (char*)workspace + tl.tape_off;
+    tp.segbuf = (char*)workspace + tl.seg_off;
+    tp.nthreads = tl.nthreads;
+    e = fp32 ? launch_tape_ck<float>(p, tp, ck, st) : launch_tape_ck<double>(p, tp, ck, st);
+  } else if (fp32) {
+    e = launch_fwdbwd_ck<float>(p, ntr, ck, st);
+  } else {
+    e = launch_fwdbwd_ck<double>(p, ntr, ck, st);
+  }
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: launch failed: %s", who, cudaGetErrorString(e));
   const int nout = cfg->nlayer + 1;
   double* ev = (double*)((char*)workspace + w.event_off);

@@ -63,12 +63,14 @@ def torch_reference(p2r, cfg, trk, hit, dr, g_trk, g_chi2, nlay=None):
                 dr=drt.grad.numpy(), bz=float(bz.grad), out_par=par.detach().numpy(), chi2=chi2.detach().numpy())
 
 
-def gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=5, nlay=None, per_event=False, fp32=False):
+def gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=5, nlay=None, per_event=False, fp32=False,
+              tape=True):
     if fp32:
         cfg = p2r.Config(**{**cfg.__dict__, "flags": cfg.flags | p2r.FLAG_ADJ_FP32})
     d = lambda a: torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).cuda()
     o = p2r.forward_backward(cfg, d(trk), d(hit), dr=d(dr), nlay_lane=None if nlay is None else d(nlay),
-                             grad_trk_out=d(g_trk), grad_chi2=d(g_chi2), ckpt_stride=ckpt, per_event=per_event)
+                             grad_trk_out=d(g_trk), grad_chi2=d(g_chi2), ckpt_stride=ckpt, per_event=per_event,
+                             tape=tape)
     torch.cuda.synchronize()
     bs = cfg.bsize
     gt = o["grad_trk_in"].cpu().numpy().reshape(cfg.nblocks, 28, bs)
@@ -127,6 +129,30 @@ def test_checkpoint_strides_agree(p2r, torch, ckpt):
     for key in ("par0", "cov0", "hpos", "hcov", "dr"):
         assert np.quantile(grad_err(other[key], base[key]), 0.999) < 1e-5, key
     assert abs(other["bz"] - base["bz"]) <= 1e-5 * abs(base["bz"])
+
+
+@pytest.mark.parametrize("ckpt", [1, 4, 5])
+@pytest.mark.parametrize("fp32", [False, True])
+def test_tape_and_thread_local_paths_identical(p2r, torch, ckpt, fp32):
+    """Checkpoints in a device-memory tape (two kernels) or in thread-local memory (one
+    kernel): the same formulas, so the same results up to where the compiler fuses a
+    multiply-add differently in the two kernels (FP64: float32 outputs all but identical),
+    with masked lanes."""
+    cfg, trk, hit, dr, g_trk, g_chi2 = setup(p2r, torch, nevts=2, nb=3, nlayer=23)
+    nlay = np.random.default_rng(3).integers(5, 24, cfg.ntracks).astype(np.int32)
+    a = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=ckpt, nlay=nlay, per_event=True, fp32=fp32)
+    b = gpu_grads(p2r, torch, cfg, trk, hit, dr, g_trk, g_chi2, ckpt=ckpt, nlay=nlay, per_event=True, fp32=fp32,
+                  tape=False)
+    for key in a:
+        x, y = np.asarray(a[key], np.float64), np.asarray(b[key], np.float64)
+        if key == "trk_out":  # the q row holds integer bits: compare par and cov rows as numbers
+            x = x.reshape(-1, 28, 32)[:, :27]
+            y = y.reshape(-1, 28, 32)[:, :27]
+        e = grad_err(x.reshape(-1), y.reshape(-1))
+        if fp32:  # FP32 gradients carry ~1e-2 of rounding (see test_fp32_adjoint_mode)
+            assert np.quantile(e, 0.99) < 2e-2, (key, np.quantile(e, [0.5, 0.99, 1]))
+        else:
+            assert np.quantile(e, 0.99) < 1e-6 and (e == 0).mean() > 0.9, (key, np.quantile(e, [0.5, 0.99, 1]))
 
 
 def test_forward_outputs_are_fp64_chain(p2r, oracle, torch):
