@@ -56,6 +56,9 @@ typedef enum p2r_mode { P2R_MODE_RESTART = 0, P2R_MODE_CHAINED = 1 } p2r_mode;
 #define P2R_FLAG_FP32_DET 0x1u   /* 2x2 residual-covariance determinant in FP32 (default FP64, TBB:457) */
 #define P2R_FLAG_NO_STAGING 0x2u /* read hits with plain loads instead of cp.async staging */
 #define P2R_FLAG_ADJ_FP32 0x4u   /* p2r_forward_backward in FP32 instead of FP64 (faster, ~1e-2 gradients) */
+#define P2R_FLAG_SQUASH_PHI 0x8u /* wrap phi into [-pi, pi] after every update: the step the reference
+                                    leaves commented out (squashPhiMPlex, TBB:635); forward entry points,
+                                    with the FP64 determinant (not with P2R_FLAG_FP32_DET) */
 
 typedef struct p2r_config {
   int32_t bsize;         /* Matriplex lanes per block (TBB:15-17); >= 1 */

@@ -25,6 +25,7 @@ MODE_CHAINED = 1
 FLAG_FP32_DET = 0x1
 FLAG_NO_STAGING = 0x2
 FLAG_ADJ_FP32 = 0x4
+FLAG_SQUASH_PHI = 0x8
 MATH_REFINED, MATH_IEEE, MATH_FAST = 0, 1, 2
 
 

@@ -543,6 +543,8 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   int rc = p2r_check_config(cfg, who);
   if (rc) return rc;
   if (cfg->mode != P2R_MODE_CHAINED) return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: only CHAINED mode has an adjoint", who);
+  if (cfg->flags & P2R_FLAG_SQUASH_PHI)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_SQUASH_PHI is a forward-only option", who);
   if (cfg->nlayer > kMaxAdjLayers)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: nlayer %d exceeds %d", who, cfg->nlayer, kMaxAdjLayers);
   const long long nblocks = (long long)cfg->nevts * cfg->nb;

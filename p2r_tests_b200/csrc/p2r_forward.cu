@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(128) propagate_kernel(const float* trk_in, con
 
 template <bool FP64DET>
 __global__ void __launch_bounds__(128) update_kernel(float* trk, const float* hits, float* chi2_accum, long long nblocks,
-                                                     int bs, int nlayer, int layer) {
+                                                     int bs, int nlayer, int layer, int squash) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long b = g / bs;
   const int it = (int)(g - b * bs);
@@ -65,6 +65,7 @@ __global__ void __launch_bounds__(128) update_kernel(float* trk, const float* hi
     chi2 = kalman_update<FP64DET, true>(par, cov, hp, hc, rh);
   else
     chi2 = kalman_update<FP64DET, false>(par, cov, hp, hc, rh);
+  if (squash) par[4] = squash_phi(par[4]);
 #pragma unroll
   for (int i = 0; i < 6; ++i) blk[i * bs + it] = par[i];
 #pragma unroll
@@ -116,6 +117,7 @@ static int forward_impl(const p2r_config* cfg, const void* trk_in, const void* h
   p.bsize = cfg->bsize;
   p.nlayer = cfg->nlayer;
   p.kfact = p2r_kfact_of(cfg->bz);
+  p.squash = (cfg->flags & P2R_FLAG_SQUASH_PHI) != 0;
   const int threads = cfg->block_threads > 0 ? cfg->block_threads : 128;
   if (threads % 32 || threads > 128)
     return p2r_set_errorf(P2R_ERR_INVALID, "%s: block_threads must be a multiple of 32 up to 128", who);
@@ -123,6 +125,8 @@ static int forward_impl(const p2r_config* cfg, const void* trk_in, const void* h
   if (stages != 2 && stages != 4) return p2r_set_errorf(P2R_ERR_INVALID, "%s: stages must be 2 or 4", who);
   const bool staged = !(cfg->flags & P2R_FLAG_NO_STAGING) && cfg->bsize % 32 == 0 && check_ptr16(hits);
   const bool fp64det = !(cfg->flags & P2R_FLAG_FP32_DET);
+  if (p.squash && !fp64det)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_SQUASH_PHI is built with the FP64 determinant only", who);
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
   if (cfg->mode == P2R_MODE_RESTART)
@@ -179,12 +183,13 @@ int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_
   const long long ntr = nblocks * cfg->bsize;
   const int threads = 128;
   const unsigned grid = (unsigned)((ntr + threads - 1) / threads);
+  const int squash = (cfg->flags & P2R_FLAG_SQUASH_PHI) != 0;
   if (cfg->flags & P2R_FLAG_FP32_DET)
     update_kernel<false><<<grid, threads, 0, (cudaStream_t)stream>>>((float*)trk, (const float*)hits, chi2_accum,
-                                                                      nblocks, cfg->bsize, cfg->nlayer, layer);
+                                                                      nblocks, cfg->bsize, cfg->nlayer, layer, squash);
   else
     update_kernel<true><<<grid, threads, 0, (cudaStream_t)stream>>>((float*)trk, (const float*)hits, chi2_accum,
-                                                                     nblocks, cfg->bsize, cfg->nlayer, layer);
+                                                                     nblocks, cfg->bsize, cfg->nlayer, layer, squash);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_kalman_update: %s", cudaGetErrorString(e));
   return p2r_clear_error();

@@ -31,6 +31,7 @@ struct FwdParams {
   int bsize;
   int nlayer;
   float kfact;
+  int squash;             // wrap phi after every update (P2R_FLAG_SQUASH_PHI)
 };
 
 constexpr int kTrkWords = 28;
@@ -80,7 +81,7 @@ __device__ __forceinline__ void store_track(float* blk, int bs, int it, const fl
 // memory). Lane `lane` owns lane `it` of block `b`; lanes run layers [0, nlay) (MASK: the
 // per-track count, else p.nlayer) and the warp iterates to its largest count. All 32 lanes
 // must call it together (bs % 32 == 0).
-template <int BS, int STAGES, bool CHI2, bool DR, bool MASK, bool FP64DET>
+template <int BS, int STAGES, bool CHI2, bool DR, bool MASK, bool FP64DET, bool SQUASH>
 __device__ __forceinline__ void chained_slice_staged(const FwdParams& p, long long b, int it, int lane, float* ring) {
   const int bs = BS > 0 ? BS : p.bsize;
   float par[6], cov[21];
@@ -117,6 +118,7 @@ __device__ __forceinline__ void chained_slice_staged(const FwdParams& p, long lo
       const float rt = DR ? rh + __ldg(p.dr + l) : rh;
       propagate_to_r(par, cov, k, kinv, rt, par, cov);
       chi2 += kalman_update<FP64DET, CHI2>(par, cov, hp, hc, rh);
+      if (SQUASH) par[4] = squash_phi(par[4]);
     }
   }
   cp_async_wait<0>();
@@ -126,7 +128,7 @@ __device__ __forceinline__ void chained_slice_staged(const FwdParams& p, long lo
 }
 
 // BS: compile-time bsize (0 = run-time p.bsize). STAGED requires bsize % 32 == 0.
-template <int BS, int STAGES, bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET>
+template <int BS, int STAGES, bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET, bool SQUASH>
 __global__ void __launch_bounds__(128) fwd_kernel(FwdParams p) {
   extern __shared__ __align__(16) float smem[];
   const int bs = BS > 0 ? BS : p.bsize;
@@ -162,6 +164,7 @@ __global__ void __launch_bounds__(128) fwd_kernel(FwdParams p) {
       float op[6], oc[21];
       propagate_to_r(par, cov, k, kinv, rt, op, oc);
       chi2 += kalman_update<FP64DET, CHI2>(op, oc, hp, hc, rh);
+      if (SQUASH) op[4] = squash_phi(op[4]);
 #pragma unroll
       for (int i = 0; i < 6; ++i) par[i] = op[i];
 #pragma unroll
@@ -196,6 +199,7 @@ __global__ void __launch_bounds__(128) fwd_kernel(FwdParams p) {
         const float rt = DR ? rh + __ldg(p.dr + l) : rh;
         propagate_to_r(par, cov, k, kinv, rt, par, cov);
         chi2 += kalman_update<FP64DET, CHI2>(par, cov, hp, hc, rh);
+        if (SQUASH) par[4] = squash_phi(par[4]);
       }
     }
     cp_async_wait<0>();
@@ -211,6 +215,7 @@ __global__ void __launch_bounds__(128) fwd_kernel(FwdParams p) {
       const float rt = DR ? rh + __ldg(p.dr + l) : rh;
       propagate_to_r(par, cov, k, kinv, rt, par, cov);
       chi2 += kalman_update<FP64DET, CHI2>(par, cov, hp, hc, rh);
+      if (SQUASH) par[4] = squash_phi(par[4]);
     }
   }
   store_track(p.trk_out + b * (long long)(kTrkWords * bs), bs, it, par, cov, q);
@@ -218,12 +223,12 @@ __global__ void __launch_bounds__(128) fwd_kernel(FwdParams p) {
 }
 
 // ---------------------------------------------------------------- launch plumbing
-template <int BS, int STAGES, bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET>
+template <int BS, int STAGES, bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET, bool SQUASH>
 inline cudaError_t launch_fwd(const FwdParams& p, int threads, cudaStream_t st) {
   const long long ntr = p.nblocks * (long long)p.bsize;
   const long long grid = (ntr + threads - 1) / threads;
   const size_t smem = STAGED ? (size_t)(threads / 32) * STAGES * 288 * sizeof(float) : 0;
-  auto kern = fwd_kernel<BS, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET>;
+  auto kern = fwd_kernel<BS, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET, SQUASH>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -233,38 +238,45 @@ inline cudaError_t launch_fwd(const FwdParams& p, int threads, cudaStream_t st) 
 }
 
 // compile-time bsize dispatch
-template <int STAGES, bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET>
+template <int STAGES, bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET, bool SQUASH>
 inline cudaError_t dispatch_bs(const FwdParams& p, int threads, cudaStream_t st) {
   switch (p.bsize) {
-    case 32: return launch_fwd<32, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET>(p, threads, st);
-    case 64: return launch_fwd<64, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET>(p, threads, st);
-    case 128: return launch_fwd<128, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET>(p, threads, st);
-    default: return launch_fwd<0, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET>(p, threads, st);
+    case 32: return launch_fwd<32, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET, SQUASH>(p, threads, st);
+    case 64: return launch_fwd<64, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET, SQUASH>(p, threads, st);
+    case 128: return launch_fwd<128, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET, SQUASH>(p, threads, st);
+    default: return launch_fwd<0, STAGES, STAGED, RESTART, CHI2, DR, MASK, FP64DET, SQUASH>(p, threads, st);
   }
 }
 
-template <bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET>
+template <bool STAGED, bool RESTART, bool CHI2, bool DR, bool MASK, bool FP64DET, bool SQUASH>
 inline cudaError_t dispatch_stages(const FwdParams& p, int threads, int stages, cudaStream_t st) {
-  if (!STAGED) return dispatch_bs<2, false, RESTART, CHI2, DR, MASK, FP64DET>(p, threads, st);
-  if (stages <= 2) return dispatch_bs<2, STAGED, RESTART, CHI2, DR, MASK, FP64DET>(p, threads, st);
-  return dispatch_bs<4, STAGED, RESTART, CHI2, DR, MASK, FP64DET>(p, threads, st);
+  if (!STAGED) return dispatch_bs<2, false, RESTART, CHI2, DR, MASK, FP64DET, SQUASH>(p, threads, st);
+  if (stages <= 2) return dispatch_bs<2, STAGED, RESTART, CHI2, DR, MASK, FP64DET, SQUASH>(p, threads, st);
+  return dispatch_bs<4, STAGED, RESTART, CHI2, DR, MASK, FP64DET, SQUASH>(p, threads, st);
 }
 
+// p.squash selects the SQUASH instances (compiled for the FP64 determinant only: a run-time
+// branch in the layer loop costs ~4 % of the chained forward).
 template <bool STAGED, bool RESTART, bool MASK>
 inline cudaError_t dispatch_flags(const FwdParams& p, bool fp64det, int threads, int stages, cudaStream_t st) {
-  const bool chi2 = p.chi2 != nullptr, dr = p.dr != nullptr;
-#define P2R_D(C, D, F) \
-  if (chi2 == C && dr == D && fp64det == F) return dispatch_stages<STAGED, RESTART, C, D, MASK, F>(p, threads, stages, st);
-  P2R_D(false, false, true)
-  P2R_D(true, false, true)
-  P2R_D(false, true, true)
-  P2R_D(true, true, true)
-  P2R_D(false, false, false)
-  P2R_D(true, false, false)
-  P2R_D(false, true, false)
-  P2R_D(true, true, false)
+  const bool chi2 = p.chi2 != nullptr, dr = p.dr != nullptr, sq = p.squash != 0;
+#define P2R_D(C, D, F, S)                        \
+  if (chi2 == C && dr == D && fp64det == F && sq == S) \
+    return dispatch_stages<STAGED, RESTART, C, D, MASK, F, S>(p, threads, stages, st);
+  P2R_D(false, false, true, false)
+  P2R_D(true, false, true, false)
+  P2R_D(false, true, true, false)
+  P2R_D(true, true, true, false)
+  P2R_D(false, false, false, false)
+  P2R_D(true, false, false, false)
+  P2R_D(false, true, false, false)
+  P2R_D(true, true, false, false)
+  P2R_D(false, false, true, true)
+  P2R_D(true, false, true, true)
+  P2R_D(false, true, true, true)
+  P2R_D(true, true, true, true)
 #undef P2R_D
-  return cudaErrorInvalidValue;
+  return cudaErrorNotSupported;
 }
 
 // Launchers, one per translation unit.

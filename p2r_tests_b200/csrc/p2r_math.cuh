@@ -307,4 +307,12 @@ __device__ __forceinline__ float kalman_update(float (&p)[6], float (&c)[21], co
   return chi2;
 }
 
+// phi wrapped into [-pi, pi]: the update step the reference leaves commented out
+// (squashPhiMPlex, TBB:635, "ensure phi is between |pi|"; the function itself is not in the
+// reference). phi - 2 pi n with n the nearest integer to phi / (2 pi), in one rounding.
+__device__ __forceinline__ float squash_phi(float phi) {
+  const float n = rintf(fmul(phi, 0.159154943f));
+  return ffma(-n, 6.28318531f, phi);
+}
+
 }  // namespace p2r

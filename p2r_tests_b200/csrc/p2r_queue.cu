@@ -46,7 +46,7 @@ __global__ void queue_init_kernel(const int64_t* ev_off, long long nevts, int sl
   }
 }
 
-template <int BS, int STAGES, bool CHI2, bool FP64DET>
+template <int BS, int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
 __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
   extern __shared__ __align__(16) float smem[];
   __shared__ int s_item;
@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
     for (int s = warp; s < nslices; s += nwarps) {
       const long long b = qi.block0 + s / spb;
       const int it = (s % spb) * 32 + lane;
-      chained_slice_staged<BS, STAGES, CHI2, false, true, FP64DET>(q.f, b, it, lane, ring);
+      chained_slice_staged<BS, STAGES, CHI2, false, true, FP64DET, SQUASH>(q.f, b, it, lane, ring);
       if (lane == 0) {
         __threadfence();
         if (atomicSub(&q.ev_remaining[qi.event], 1) == 1 && q.ev_done) q.ev_done[qi.event] = globaltimer_ns();
@@ -75,9 +75,9 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
   }
 }
 
-template <int BS, int STAGES, bool CHI2, bool FP64DET>
+template <int BS, int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
 cudaError_t launch_queue_t(const QueueParams& q, int threads, int ctas_per_sm, cudaStream_t st) {
-  auto kern = queue_kernel<BS, STAGES, CHI2, FP64DET>;
+  auto kern = queue_kernel<BS, STAGES, CHI2, FP64DET, SQUASH>;
   const size_t smem = (size_t)(threads / 32) * STAGES * 288 * sizeof(float);
   int dev = 0, sms = 0, occ = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -91,13 +91,13 @@ cudaError_t launch_queue_t(const QueueParams& q, int threads, int ctas_per_sm, c
   return cudaGetLastError();
 }
 
-template <int STAGES, bool CHI2, bool FP64DET>
+template <int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
 cudaError_t launch_queue_bs(const QueueParams& q, int threads, int ctas, cudaStream_t st) {
   switch (q.f.bsize) {
-    case 32: return launch_queue_t<32, STAGES, CHI2, FP64DET>(q, threads, ctas, st);
-    case 64: return launch_queue_t<64, STAGES, CHI2, FP64DET>(q, threads, ctas, st);
-    case 128: return launch_queue_t<128, STAGES, CHI2, FP64DET>(q, threads, ctas, st);
-    default: return launch_queue_t<0, STAGES, CHI2, FP64DET>(q, threads, ctas, st);
+    case 32: return launch_queue_t<32, STAGES, CHI2, FP64DET, SQUASH>(q, threads, ctas, st);
+    case 64: return launch_queue_t<64, STAGES, CHI2, FP64DET, SQUASH>(q, threads, ctas, st);
+    case 128: return launch_queue_t<128, STAGES, CHI2, FP64DET, SQUASH>(q, threads, ctas, st);
+    default: return launch_queue_t<0, STAGES, CHI2, FP64DET, SQUASH>(q, threads, ctas, st);
   }
 }
 
@@ -135,6 +135,8 @@ int check_queue(const p2r_queue* q, const char* who) {
   if (q->stages != 0 && q->stages != 2 && q->stages != 4)
     return p2r_set_errorf(P2R_ERR_INVALID, "%s: stages must be 2 or 4", who);
   if (!std::isfinite(q->bz)) return p2r_set_errorf(P2R_ERR_INVALID, "%s: bz is not finite", who);
+  if ((q->flags & P2R_FLAG_SQUASH_PHI) && (q->flags & P2R_FLAG_FP32_DET))
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_SQUASH_PHI is built with the FP64 determinant only", who);
   return P2R_OK;
 }
 
@@ -161,6 +163,7 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
   qp.f.bsize = q->bsize;
   qp.f.nlayer = q->nlayer;
   qp.f.kfact = p2r_kfact_of(q->bz);
+  qp.f.squash = (q->flags & P2R_FLAG_SQUASH_PHI) != 0;
   qp.items = q->items;
   qp.n_items = q->n_items;
   qp.counter = (int*)((char*)workspace + w.counter_off);
@@ -175,16 +178,25 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
     const int stages = q->stages > 0 ? q->stages : 4;
     const bool fp64 = !(q->flags & P2R_FLAG_FP32_DET);
     const bool chi2 = chi2_out != nullptr;
-    if (stages == 2)
-      e = chi2 ? (fp64 ? launch_queue_bs<2, true, true>(qp, threads, q->ctas_per_sm, st)
-                       : launch_queue_bs<2, true, false>(qp, threads, q->ctas_per_sm, st))
-               : (fp64 ? launch_queue_bs<2, false, true>(qp, threads, q->ctas_per_sm, st)
-                       : launch_queue_bs<2, false, false>(qp, threads, q->ctas_per_sm, st));
-    else
-      e = chi2 ? (fp64 ? launch_queue_bs<4, true, true>(qp, threads, q->ctas_per_sm, st)
-                       : launch_queue_bs<4, true, false>(qp, threads, q->ctas_per_sm, st))
-               : (fp64 ? launch_queue_bs<4, false, true>(qp, threads, q->ctas_per_sm, st)
-                       : launch_queue_bs<4, false, false>(qp, threads, q->ctas_per_sm, st));
+    const int c = q->ctas_per_sm;
+    if (qp.f.squash && !fp64) {
+      e = cudaErrorNotSupported;  // rejected before launch in p2r_run_queue's checks
+    } else if (qp.f.squash) {
+      e = stages == 2 ? (chi2 ? launch_queue_bs<2, true, true, true>(qp, threads, c, st)
+                              : launch_queue_bs<2, false, true, true>(qp, threads, c, st))
+                      : (chi2 ? launch_queue_bs<4, true, true, true>(qp, threads, c, st)
+                              : launch_queue_bs<4, false, true, true>(qp, threads, c, st));
+    } else if (stages == 2) {
+      e = chi2 ? (fp64 ? launch_queue_bs<2, true, true, false>(qp, threads, c, st)
+                       : launch_queue_bs<2, true, false, false>(qp, threads, c, st))
+               : (fp64 ? launch_queue_bs<2, false, true, false>(qp, threads, c, st)
+                       : launch_queue_bs<2, false, false, false>(qp, threads, c, st));
+    } else {
+      e = chi2 ? (fp64 ? launch_queue_bs<4, true, true, false>(qp, threads, c, st)
+                       : launch_queue_bs<4, true, false, false>(qp, threads, c, st))
+               : (fp64 ? launch_queue_bs<4, false, true, false>(qp, threads, c, st)
+                       : launch_queue_bs<4, false, false, false>(qp, threads, c, st));
+    }
   }
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: launch failed: %s", who, cudaGetErrorString(e));
   return p2r_clear_error();

@@ -95,3 +95,20 @@ def test_generators_reject_bad_args(p2r):
     buf = np.zeros(100, np.float32)
     assert l.p2r_gen_fixture(buf.ctypes.data, buf.ctypes.data, 1, buf.ctypes.data, 2, 32, 1, 1, 20, 1e-5,
                              buf.ctypes.data, buf.ctypes.data) == 1  # nlayer > input hits
+
+
+def test_adjoint_rejects_forward_only_options(p2r):
+    """squash-phi is a forward-only option; the adjoint refuses it before any device work,
+    and the tape workspace size grows with the tape and is reported for valid strides only."""
+    l = p2r.lib()
+    c = _cfg(p2r, flags=p2r.FLAG_SQUASH_PHI)
+    rc = l.p2r_forward_backward(ctypes.byref(c), 16, 32, None, None, 48, None, None, None, None, None, None, None,
+                                None, None, 5, 256, 1 << 20, None)
+    assert rc == 4 and "SQUASH" in l.p2r_last_error_string().decode()
+    c = _cfg(p2r, nevts=10, nb=30)
+    small = l.p2r_forward_backward_workspace_size(ctypes.byref(c))
+    tape1 = l.p2r_forward_backward_workspace_size_tape(ctypes.byref(c), 1)
+    tape5 = l.p2r_forward_backward_workspace_size_tape(ctypes.byref(c), 5)
+    assert small < tape5 < tape1
+    assert tape1 >= small + 20 * 27 * 8 * 10 * 30 * 32  # 20 FP64 checkpoints per track
+    assert l.p2r_forward_backward_workspace_size_tape(ctypes.byref(c), 3) == 0

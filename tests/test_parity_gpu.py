@@ -227,6 +227,32 @@ def test_staged_equals_plain_loads(p2r, torch, bs):
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), "staged vs plain loads"
 
 
+@pytest.mark.parametrize("mode", ["restart", "chained"])
+def test_squash_phi_option(p2r, torch, mode):
+    """P2R_FLAG_SQUASH_PHI (the reference's commented-out squashPhiMPlex, TBB:635): phi stays in
+    [-pi, pi] and equals the unwrapped phi modulo 2 pi; the other parameters agree to the
+    parity tolerance (a wrapped phi changes the rounding of the next sin/cos), and the fused
+    and per-layer paths give identical results with the option."""
+    cfg, trk, hit = helix(p2r, 4, 30)
+    cfg.mode = MODES[mode]
+    a = gpu_forward(p2r, torch, cfg, trk, hit)
+    cfg.flags = p2r.FLAG_SQUASH_PHI
+    b = gpu_forward(p2r, torch, cfg, trk, hit)
+    pa, pb = parity.unpack(a, 32)[0], parity.unpack(b, 32)[0]
+    assert (np.abs(pb[:, 4]) <= np.pi + 1e-6).all()
+    d = np.remainder(pa[:, 4] - pb[:, 4] + np.pi, 2 * np.pi) - np.pi
+    assert np.abs(d).max() < 1e-4
+    if mode == "chained":
+        assert (np.abs(pa[:, 4]) > np.pi).sum() > 0  # some tracks crossed phi = +-pi
+    other = [0, 1, 2, 3, 5]
+    assert np.quantile(parity.rel_par(pb, pa)[:, other], 0.999) < parity.PAR_RTOL
+    dt, dh = dev(torch, trk), dev(torch, hit)
+    out = torch.empty_like(dt)
+    p2r.run_layers(cfg, dt, dh, out)
+    torch.cuda.synchronize()
+    assert np.array_equal(host(out).view(np.uint32), b.view(np.uint32))
+
+
 @pytest.mark.parametrize("threads,stages", [(32, 2), (64, 4), (96, 4), (128, 2)])
 def test_launch_shapes_identical(p2r, torch, threads, stages):
     """The same kernel instantiation under another launch shape is bit-identical."""

@@ -61,18 +61,21 @@ def small_batch(p2r):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("g", [1, 4, 16])
-def test_queue_matches_masked_forward(p2r, torch, small_batch, g):
+@pytest.mark.parametrize("g,flags", [(1, 0), (4, 0), (16, 0), (4, "squash")])
+def test_queue_matches_masked_forward(p2r, torch, small_batch, g, flags):
+    """The persistent queue performs the masked fused forward's operations: bit-identical
+    (also with phi wrapped after every update)."""
     w = small_batch
-    q = p2r.Queue(w, blocks_per_item=g)
+    fl = p2r.FLAG_SQUASH_PHI if flags == "squash" else 0
+    q = p2r.Queue(w, blocks_per_item=g, flags=fl)
     t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
     out = torch.empty_like(t)
     q.run(t, h, out)
-    cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"])
+    cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"], flags=fl)
     ref = torch.empty_like(t)
     p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
     torch.cuda.synchronize()
-    parity.assert_same_arithmetic(out.cpu().numpy(), ref.cpu().numpy(), 32, f"queue G={g} vs masked forward")
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32)), (g, flags)
     lat = q.event_latency_ns()
     assert (lat > 0).all() and (lat < 10_000_000_000).all()
 
