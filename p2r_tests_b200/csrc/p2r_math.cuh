@@ -131,37 +131,38 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
     const float id = fsub(r, r0);
     D = fadd(D, id);
     sincos4(fmul(id, ik), sina, omc);
+    // momentum direction after the step: (px ca - py sa, py ca + px sa)
+    const float pxca = mulcos(pxin, omc), pyca = mulcos(pyin, omc);
+    const float a1 = ffma(-pyin, sina, pxca);
+    const float a2 = ffma(pxin, sina, pyca);
     // Path derivatives, only once the step is below 1 um (TBB:714). The reference scales every
     // derivative increment by oor0 = 0 until then; adding a finite x * 0 leaves the sums
     // unchanged, so those increments are skipped.
     if (i + 1 != 5 && r0 > 0.f && fabsf(id) < 0.0001f) {
       const float noor0 = -fdiv(1.f, r0);  // -1/r0
-      const float kn = fmul(iptin, noor0);
-      const float tx = fmul(xo, kn), ty = fmul(yo, kn);  // k*dadx, k*dady of TBB:716-717
-      const float pxca = mulcos(pxin, omc), pxsa = fmul(pxin, sina);
-      const float pyca = mulcos(pyin, omc), pysa = fmul(pyin, sina);
-      const float a1 = fsub(pxca, pysa);
-      const float a2 = fadd(pyca, pxsa);
-      // dDdx -= (xo*(1 + tx*a1) + yo*tx*a2) * oor0
-      dDdx = ffma(ffma(xo, ffma(tx, a1, 1.f), fmul(fmul(yo, tx), a2)), noor0, dDdx);
-      // dDdy -= (xo*ty*a1 + yo*(1 + ty*a2)) * oor0
-      dDdy = ffma(ffma(yo, ffma(ty, a2, 1.f), fmul(fmul(xo, ty), a1)), noor0, dDdy);
-      // dDdipt -= k*(xo*(pxca*t - pysa*t - pyca - pxsa + pyin)
-      //             + yo*(pyca*t + pxsa*t - pysa + pxca - pxin)) * pt * oor0,  t = dadipt*ipt
+      const float kn = fmul(iptin, noor0);  // k*dadx/xo = k*dady/yo of TBB:716-717
+      // dDdx -= (xo*(1 + tx*a1) + yo*tx*a2) * oor0 and dDdy -= (xo*ty*a1 + yo*(1 + ty*a2)) * oor0
+      // with tx = kn*xo, ty = kn*yo: xo resp. yo times (1 + kn*(xo*a1 + yo*a2)) * oor0
+      const float g = fmul(ffma(kn, ffma(xo, a1, fmul(yo, a2)), 1.f), noor0);
+      dDdx = ffma(xo, g, dDdx);
+      dDdy = ffma(yo, g, dDdy);
+      // dDdipt -= k*(xo*e1 + yo*e2)*pt*oor0 with t = dadipt*ipt,
+      //   e1 = pxca*t - pysa*t - pyca - pxsa + pyin = a1*t + (pyin - a2)
+      //   e2 = pyca*t + pxsa*t - pysa + pxca - pxin = a2*t + (a1 - pxin)
       const float t = fmul(id, ik);
-      const float e1 = ffma(a1, t, fsub(pyin, a2));
+      const float u = fsub(pyin, a2);
+      const float e1 = ffma(a1, t, u);
       const float e2 = ffma(a2, t, fsub(a1, pxin));
       dDdipt = ffma(ffma(xo, e1, fmul(yo, e2)), fmul(kpt, noor0), dDdipt);
       // dDdphi += k*(xo*(pysa - pxin + pxca) - yo*(pxsa - pyin + pyca)) * oor0
-      const float f1 = fadd(fsub(pysa, pxin), pxca);
-      const float nf2 = fsub(fsub(pyin, pxsa), pyca);
-      dDdphi = ffma(ffma(yo, nf2, fmul(xo, f1)), fmul(-k, noor0), dDdphi);
+      //         = k*(xo*f1 + yo*u) * oor0,  f1 = pyin*sina + pxca - pxin
+      const float f1 = fsub(ffma(pyin, sina, pxca), pxin);
+      dDdphi = ffma(ffma(yo, u, fmul(xo, f1)), fmul(-k, noor0), dDdphi);
     }
     xo = ffma(k, ffma(pxin, sina, fmul(-pyin, omc)), xo);  // xo + k*(pxin*sina - pyin*omc)
     yo = ffma(k, ffma(pyin, sina, fmul(pxin, omc)), yo);   // yo + k*(pyin*sina + pxin*omc)
-    const float pxold = pxin;
-    pxin = ffma(-pyin, sina, mulcos(pxin, omc));  // pxin*cosa - pyin*sina
-    pyin = ffma(pxold, sina, mulcos(pyin, omc));  // pyin*cosa + pxin*sina
+    pxin = a1;
+    pyin = a2;
   }
 
   const float alpha = fmul(D, ik);
