@@ -8,8 +8,10 @@
 // The reference evaluates these per Matriplex block with one SIMD loop per stage and
 // materialises the 6x6 Jacobian, J*C and K*H*C in memory. Here one thread owns one track: the
 // 6 parameters and 21 covariance elements stay in registers across layers, the Jacobian is a
-// set of 17 scalars (its unit rows 3 and 5 and its structural zeros are never formed), and
-// J*C, (J*C)*J^T and C - K*(H*C) are expanded at compile time over the non-zero terms.
+// set of scalars (its unit rows 3 and 5 and its structural zeros are never formed, and rows 2
+// and 4, which share the factors dadx, dady, dadphi, are applied through one shared
+// combination), and J*C, (J*C)*J^T and C - K*(H*C) are expanded at compile time over the
+// non-zero terms.
 //
 // Every multiply, add and fused multiply-add is written out (fmul / fadd / fsub / ffma, all
 // round-to-nearest, never re-associated or contracted by the compiler), so every kernel that
@@ -197,12 +199,15 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
   const float isinT = fdiv(1.f, sinT);
   const float kpi = fmul(kpt, isinT);  // k*pt/sinT
   const float kpc = fmul(kpi, cosT);   // k*pt*cosT/sinT
-  const float J20 = fmul(dadx, kpc);
-  const float J21 = fmul(dady, kpc);
+  // rows 2 and 4 share (dadx, dady, ., ., dadphi, .): J2 = kpc*(dadx, dady, 0, 0, dadphi, 0)
+  // + (0, 0, 1, J23, 0, J25) and J4 = (dadx, dady, 0, dadipt, 1 + dadphi, 0), so for a vector v
+  // with n = dadx*v0 + dady*v1 + dadphi*v4: v.J2 = kpc*n + v2 + J23*v3 + J25*v5 and
+  // v.J4 = n + dadipt*v3 + v4
   const float J23 = fmul(fmul(fsub(ia, alpha), kpc), pt);
-  const float J24 = fmul(dadphi, kpc);
   const float J25 = fmul(fmul(-alpha, kpi), isinT);  // -k*alpha*pt/sinT^2
-  const float J40 = dadx, J41 = dady, J43 = dadipt, J44 = fadd(1.f, dadphi);
+  auto nvec = [&](float v0, float v1, float v4) { return ffma(dadphi, v4, ffma(dady, v1, fmul(dadx, v0))); };
+  auto dotJ2 = [&](float n, float v2, float v3, float v5) { return ffma(kpc, n, ffma(J25, v5, ffma(J23, v3, v2))); };
+  auto dotJ4 = [&](float n, float v3, float v4) { return fadd(ffma(dadipt, v3, n), v4); };
 
   // T = J*C (TBB:296-341): rows 3 and 5 of T are rows 3 and 5 of C.
   float T0[6], T1[6], T2[6], T4[6];
@@ -212,8 +217,9 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
     const float c3 = ic[S6(3, j)], c4 = ic[S6(4, j)], c5 = ic[S6(5, j)];
     T0[j] = ffma(J04, c4, ffma(J03, c3, ffma(J01, c1, fmul(J00, c0))));
     T1[j] = ffma(J14, c4, ffma(J13, c3, ffma(J11, c1, fmul(J10, c0))));
-    T2[j] = ffma(J25, c5, ffma(J24, c4, ffma(J23, c3, fadd(ffma(J21, c1, fmul(J20, c0)), c2))));
-    T4[j] = ffma(J44, c4, ffma(J43, c3, ffma(J41, c1, fmul(J40, c0))));
+    const float n = nvec(c0, c1, c4);
+    T2[j] = dotJ2(n, c2, c3, c5);
+    T4[j] = dotJ4(n, c3, c4);
   }
   float T3[6], T5[6];
 #pragma unroll
@@ -224,16 +230,17 @@ __device__ __forceinline__ void propagate_to_r(const float (&ip)[6], const float
 
   // C' = T*J^T, lower triangle (TBB:343-373).
   float nc[21];
-#define P2R_ROW(i, Ti)                                                                                           \
-  {                                                                                                              \
-    nc[S6(i, 0)] = ffma(Ti[4], J04, ffma(Ti[3], J03, ffma(Ti[1], J01, fmul(Ti[0], J00))));                        \
-    if (i >= 1) nc[S6(i, 1)] = ffma(Ti[4], J14, ffma(Ti[3], J13, ffma(Ti[1], J11, fmul(Ti[0], J10))));            \
-    if (i >= 2)                                                                                                  \
-      nc[S6(i, 2)] =                                                                                             \
-          ffma(Ti[5], J25, ffma(Ti[4], J24, ffma(Ti[3], J23, fadd(ffma(Ti[1], J21, fmul(Ti[0], J20)), Ti[2])))); \
-    if (i >= 3) nc[S6(i, 3)] = Ti[3];                                                                            \
-    if (i >= 4) nc[S6(i, 4)] = ffma(Ti[4], J44, ffma(Ti[3], J43, ffma(Ti[1], J41, fmul(Ti[0], J40))));            \
-    if (i >= 5) nc[S6(i, 5)] = Ti[5];                                                                            \
+#define P2R_ROW(i, Ti)                                                                                \
+  {                                                                                                   \
+    nc[S6(i, 0)] = ffma(Ti[4], J04, ffma(Ti[3], J03, ffma(Ti[1], J01, fmul(Ti[0], J00))));             \
+    if (i >= 1) nc[S6(i, 1)] = ffma(Ti[4], J14, ffma(Ti[3], J13, ffma(Ti[1], J11, fmul(Ti[0], J10)))); \
+    if (i >= 2) {                                                                                     \
+      const float n = nvec(Ti[0], Ti[1], Ti[4]);                                                      \
+      nc[S6(i, 2)] = dotJ2(n, Ti[2], Ti[3], Ti[5]);                                                   \
+      if (i >= 4) nc[S6(i, 4)] = dotJ4(n, Ti[3], Ti[4]);                                              \
+    }                                                                                                 \
+    if (i >= 3) nc[S6(i, 3)] = Ti[3];                                                                 \
+    if (i >= 5) nc[S6(i, 5)] = Ti[5];                                                                 \
   }
   P2R_ROW(0, T0)
   P2R_ROW(1, T1)
