@@ -380,3 +380,30 @@ def test_full_size_chained_sample_vs_reference(p2r, oracle, torch):
     got = out.reshape(cfg.nblocks, 28, 32)[sel]
     f64 = oracle.run(t_s, h_s, 32, cfg.nlayer, 1, cfg.bz, "f64")
     parity.assert_accuracy_parity(got, want, f64["par"], f64["cov"], f64["prior"], 32, "full size sample")
+
+
+def test_arrays_beyond_32_bit_offsets(p2r, torch):
+    """A batch whose hit array has more than 2^31 elements (60 events x 1e5 tracks x 40 layers,
+    8.6 GB, generated on the device): the tracks of the last event, whose hit offsets need 64
+    bits, come out bit-identical to the same event run alone, for the fused forward and the
+    masked forward."""
+    nevts, nb, nl = 60, 3125, 40
+    cfg = p2r.Config(bsize=32, nlayer=nl, nevts=nevts, nb=nb, bz=3.8)
+    gp = p2r.gen_params(bz=3.8, seed=777, r_first=4.0, r_last=110.0)
+    trk, hit = p2r.generate_helix_device(cfg, gp)
+    assert hit.numel() > 2**31
+    out = torch.empty_like(trk)
+    p2r.forward(cfg, trk, hit, out)
+    per_t, per_h = trk.numel() // nevts, hit.numel() // nevts
+    one = p2r.Config(bsize=32, nlayer=nl, nevts=1, nb=nb, bz=3.8)
+    t1, h1 = trk[-per_t:].clone(), hit[-per_h:].clone()
+    o1 = torch.empty_like(t1)
+    p2r.forward(one, t1, h1, o1)
+    assert torch.equal(out[-per_t:].view(torch.int32), o1.view(torch.int32))
+    nlay = torch.randint(1, nl + 1, (cfg.ntracks,), dtype=torch.int32, device="cuda",
+                         generator=torch.Generator("cuda").manual_seed(5))
+    p2r.forward(cfg, trk, hit, out, nlay_lane=nlay)
+    p2r.forward(one, t1, h1, o1, nlay_lane=nlay[-nb * 32:].clone())
+    torch.cuda.synchronize()
+    assert torch.equal(out[-per_t:].view(torch.int32), o1.view(torch.int32))
+    del trk, hit, out
