@@ -100,7 +100,7 @@ __device__ __forceinline__ float det_recip_fp64(float e0, float e1, float e2) {
 // written, the chained filter loses about a factor 2.5 in accuracy on 1/pT).
 __device__ __forceinline__ void sincos4(float x, float& s, float& omc) {
   const float x2 = fmul(x, x);
-  omc = ffma(fmul(-0.04166667f, x2), x2, fmul(0.5f, x2));
+  omc = fmul(x2, ffma(-0.04166667f, x2, 0.5f));
   s = ffma(fmul(-0.16666667f, x), x2, x);
 }
 __device__ __forceinline__ float mulcos(float v, float omc) { return ffma(-v, omc, v); }  // v*cos
