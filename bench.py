@@ -388,7 +388,29 @@ def main():
         torch.cuda.synchronize()
         gms = g0.elapsed_time(g1) / args.uneven_steps
         lat = q.event_latency_ns() / 1e6
+        qref = qo.cpu().numpy()
         q.release()
+        # the same tracks ordered by layer count within each event (p2r.sort_by_layers): warps
+        # of tracks with similar lengths idle less; per-track results are bit-identical
+        ws_, perm = p2r.sort_by_layers(w)
+        qs = p2r.Queue(ws_, blocks_per_item=tq["blocks_per_item"], block_threads=tq["block_threads"],
+                       stages=tq["stages"])
+        st_, sh_ = torch.from_numpy(ws_["trk"].reshape(-1)).to(dev), torch.from_numpy(ws_["hit"].reshape(-1)).to(dev)
+        so_ = torch.empty_like(st_)
+        qs.capture(st_, sh_, so_)
+        for _ in range(3):
+            qs.replay(stream)
+        torch.cuda.synchronize()
+        g0.record(stream)
+        for _ in range(args.uneven_steps):
+            qs.replay(stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        sms = g0.elapsed_time(g1) / args.uneven_steps
+        back = p2r.permute_tracks(so_.cpu().numpy(), p2r.inverse(perm), tq["bsize"], 28)
+        same = bool(np.array_equal(back.view(np.uint32).reshape(-1), qref.view(np.uint32).reshape(-1)))
+        qs.release()
+        del st_, sh_, so_, ws_
         uneven = {"workload": "1000 events, tracks/event log-normal (median 2000, sigma 1.0) clipped to "
                               "[50, 20000], layers/track uniform 10..25, chained",
                   "tracks": int(counts.sum()), "updates": w["updates"], "bsize": tq["bsize"],
@@ -396,7 +418,10 @@ def main():
                   "stages": tq["stages"], "ms_per_step": gms, "updates_per_s": w["updates"] / (gms / 1e3),
                   "p50_event_ms": float(np.percentile(lat, 50)), "p99_event_ms": float(np.percentile(lat, 99)),
                   "launch": "CUDA graph (queue init + one persistent kernel)", "steps": args.uneven_steps,
-                  "autotune_candidates": len(tq["tried"])}
+                  "autotune_candidates": len(tq["tried"]),
+                  "sorted_by_layer_count": {"ms_per_step": sms, "updates_per_s": w["updates"] / (sms / 1e3),
+                                            "outputs_identical_per_track": same,
+                                            "how": "each event's tracks ordered by layer count (p2r.sort_by_layers)"}}
         del qt, qh, qo, wl
 
     # calibration workload: 1e5 tracks x 100 events x 40 layers (r = 4..110 cm), generated on
@@ -426,7 +451,18 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         fms = f0.elapsed_time(f1) / args.calib_steps
-        del o4
+        # the same tracks ordered by layer count within each event (fewer idle lanes per warp)
+        t4s, h4s, nl4s, _ = p2r.sort_by_layers_device(c4, t4, h4, nl4)
+        for _ in range(2):
+            p2r.forward(c4, t4s, h4s, o4, dr=dr4, nlay_lane=nl4s, stream=stream)
+        torch.cuda.synchronize()
+        f0.record(stream)
+        for _ in range(args.calib_steps):
+            p2r.forward(c4, t4s, h4s, o4, dr=dr4, nlay_lane=nl4s, stream=stream)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fms_sorted = f0.elapsed_time(f1) / args.calib_steps
+        del o4, t4s, h4s, nl4s
         gc4 = torch.ones(c4.ntracks, dtype=torch.float32, device=dev)
         out4 = {"grad_trk_in": None, "grad_hits": None}
         p2r.forward_backward(c4, t4, h4, dr=dr4, nlay_lane=nl4, grad_chi2=gc4, per_event=True, out=out4,
@@ -452,7 +488,9 @@ def main():
                  "hits_bytes": h4.numel() * 4, "tracks_bytes": t4.numel() * 4, "updates": upd4,
                  "device_generation_ms": gen0.elapsed_time(gen1),
                  "forward": {"ms_per_step": fms, "updates_per_s": upd4 / (fms / 1e3),
-                             "api": "p2r_forward_masked (fused, per-track layer counts)"},
+                             "api": "p2r_forward_masked (fused, per-track layer counts)",
+                             "sorted_by_layer_count": {"ms_per_step": fms_sorted,
+                                                       "updates_per_s": upd4 / (fms_sorted / 1e3)}},
                  "forward_adjoint": {"ms_per_step": bms, "ratio_vs_forward": bms / fms,
                                      "api": "p2r_forward_backward (FP64, ckpt 5), per-event grad_dr/grad_bz, "
                                             "replayed from one CUDA graph"},

@@ -42,6 +42,61 @@ def uneven_workload(ntrk_event, bsize: int = 32, nlayer_max: int = 25, lay_lo: i
                 nblocks=nblocks, bsize=bsize, nlayer=nlayer_max, bz=bz, updates=int(nlay.sum()))
 
 
+def permute_tracks(arr: np.ndarray, perm: np.ndarray, bsize: int, words: int, nlayer: int = 1) -> np.ndarray:
+    """Matriplex array (tracks: words=28, nlayer=1; hits: words=9, nlayer layers per block)
+    with its tracks reordered: track i of the result is track perm[i] of arr."""
+    a = np.ascontiguousarray(arr).reshape(-1, nlayer, words, bsize)
+    nblocks = a.shape[0]
+    t = a.transpose(0, 3, 1, 2).reshape(nblocks * bsize, nlayer, words)[perm]
+    return np.ascontiguousarray(t.reshape(nblocks, bsize, nlayer, words).transpose(0, 2, 3, 1)).reshape(arr.shape)
+
+
+def sort_by_layers(w: dict) -> tuple[dict, np.ndarray]:
+    """The same uneven workload with each event's tracks ordered by layer count, longest first.
+
+    A warp runs until the longest of its 32 tracks is done, so with layer counts spread over
+    10-25 about a third of the lanes idle at the end; grouping tracks of similar length in the
+    same 32-lane slices keeps them busy. Events stay where they are (padding lanes, which have
+    no layers, stay at the end of their event), and every track's result is bit-identical in
+    either order. Returns (workload, perm): track i of the new arrays is track perm[i] of the
+    old ones; permute_tracks(out, inverse(perm), ...) puts outputs back in the old order."""
+    bs, nl = w["bsize"], w["nlayer"]
+    off = np.asarray(w["event_block_offset"], np.int64)
+    nlay = np.asarray(w["nlay_lane"])
+    perm = np.arange(w["nblocks"] * bs)
+    for e in range(len(off) - 1):
+        a, b = off[e] * bs, off[e + 1] * bs
+        perm[a:b] = a + np.argsort(-nlay[a:b], kind="stable")
+    out = dict(w)
+    out["trk"] = permute_tracks(w["trk"], perm, bs, 28)
+    out["hit"] = permute_tracks(w["hit"], perm, bs, 9, nl)
+    out["nlay_lane"] = np.ascontiguousarray(nlay[perm])
+    return out, perm
+
+
+def sort_by_layers_device(cfg: Config, trk, hits, nlay_lane):
+    """sort_by_layers for device arrays of cfg's regular layout (nevts events of nb blocks):
+    returns (trk, hits, nlay_lane, perm) as new device tensors, each event's tracks ordered by
+    layer count, longest first; perm[i] is the old index of new track i."""
+    import torch
+    bs, nl, nblocks = cfg.bsize, cfg.nlayer, cfg.nblocks
+    n = nblocks * bs
+    ev = torch.arange(n, device=nlay_lane.device, dtype=torch.int64) // (cfg.nb * bs)
+    key = ev * (nl + 2) + (nl - nlay_lane.to(torch.int64).clamp(0, nl))
+    perm = torch.argsort(key, stable=True)
+    t = trk.view(nblocks, 28, bs).permute(0, 2, 1).reshape(n, 28)[perm]
+    t = t.reshape(nblocks, bs, 28).permute(0, 2, 1).contiguous().view(-1)
+    h = hits.view(nblocks, nl, 9, bs).permute(0, 3, 1, 2).reshape(n, nl, 9)[perm]
+    h = h.reshape(nblocks, bs, nl, 9).permute(0, 2, 3, 1).contiguous().view(-1)
+    return t, h, nlay_lane[perm].contiguous(), perm
+
+
+def inverse(perm: np.ndarray) -> np.ndarray:
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm))
+    return inv
+
+
 def plan(event_block_offset: np.ndarray, blocks_per_item: int) -> np.ndarray:
     """Work items (event, nblk, block0) as a structured numpy array."""
     off = np.ascontiguousarray(event_block_offset, np.int64)

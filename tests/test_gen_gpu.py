@@ -43,3 +43,27 @@ def test_device_generator_empty_and_invalid():
     p2r.generate_helix_device(cfg)  # empty batch: no launch
     with pytest.raises(p2r.P2RError):
         p2r.generate_helix_device(p2r.Config(bsize=32, nlayer=20, nevts=1, nb=1, bz=0.0))
+
+
+def test_device_sort_by_layers_matches_host():
+    """sort_by_layers_device orders each event's tracks like the host sort_by_layers, and the
+    masked forward on the sorted arrays gives each track its unsorted result bit for bit."""
+    import torch
+    import p2r_tests_b200 as p2r
+    cfg = p2r.Config(bsize=32, nlayer=12, nevts=3, nb=4, bz=3.8)
+    trk, hit = p2r.generate_helix_device(cfg)
+    nlay = torch.randint(1, 13, (cfg.ntracks,), dtype=torch.int32, device="cuda",
+                         generator=torch.Generator("cuda").manual_seed(2))
+    ts, hs, ns, perm = p2r.sort_by_layers_device(cfg, trk, hit, nlay)
+    w = dict(trk=trk.cpu().numpy().reshape(cfg.nblocks, 28, 32), hit=hit.cpu().numpy(),
+             nlay_lane=nlay.cpu().numpy(), event_block_offset=np.arange(cfg.nevts + 1) * cfg.nb, bsize=32,
+             nlayer=cfg.nlayer, nblocks=cfg.nblocks)
+    wh, ph = p2r.sort_by_layers(w)
+    assert np.array_equal(perm.cpu().numpy(), ph)
+    bits = lambda a: np.ascontiguousarray(a).reshape(-1).view(np.uint32)
+    assert np.array_equal(bits(ts.cpu().numpy()), bits(wh["trk"])) and np.array_equal(bits(hs.cpu().numpy()), bits(wh["hit"]))
+    a, b = torch.empty_like(trk), torch.empty_like(trk)
+    p2r.forward(cfg, trk, hit, a, nlay_lane=nlay)
+    p2r.forward(cfg, ts, hs, b, nlay_lane=ns)
+    back = p2r.permute_tracks(b.cpu().numpy(), p2r.inverse(ph), 32, 28)
+    assert np.array_equal(bits(back), bits(a.cpu().numpy()))

@@ -42,6 +42,25 @@ def test_uneven_workload_padding(p2r):
     assert w["updates"] == int(nl.sum())
 
 
+def test_sort_by_layers_permutation(p2r):
+    """Ordering by layer count permutes tracks within events only, longest first, and
+    permute_tracks with the inverse restores the arrays exactly."""
+    w = p2r.uneven_workload(p2r.lognormal_counts(6, median=70, sigma=0.8, lo=5, hi=300, seed=5), bsize=32)
+    ws, perm = p2r.sort_by_layers(w)
+    off = w["event_block_offset"] * 32
+    for e in range(len(off) - 1):
+        seg = perm[off[e]:off[e + 1]]
+        assert seg.min() >= off[e] and seg.max() < off[e + 1]
+        nl = ws["nlay_lane"][off[e]:off[e + 1]]
+        assert (np.diff(nl) <= 0).all()
+    inv = p2r.inverse(perm)
+    bits = lambda a: np.ascontiguousarray(a).view(np.uint32)  # the q row holds integer bits
+    assert np.array_equal(bits(p2r.permute_tracks(ws["trk"], inv, 32, 28)), bits(w["trk"]))
+    assert np.array_equal(bits(p2r.permute_tracks(ws["hit"], inv, 32, 9, w["nlayer"])), bits(w["hit"]))
+    assert np.array_equal(ws["nlay_lane"][inv], w["nlay_lane"])
+    assert int(ws["nlay_lane"].sum()) == w["updates"]
+
+
 # ------------------------------------------------------------------------------- GPU
 @pytest.fixture(scope="module")
 def torch():
@@ -117,6 +136,23 @@ def test_queue_matches_reference(p2r, oracle, torch, small_batch):
     a = got.reshape(-1, 28, 32).transpose(0, 2, 1).reshape(-1, 28)[pad]
     b = w["trk"].reshape(-1, 28, 32).transpose(0, 2, 1).reshape(-1, 28)[pad]
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_queue_sorted_by_layers_same_results(p2r, torch, small_batch):
+    """The same tracks ordered by layer count give bit-identical results per track."""
+    w = small_batch
+    ws, perm = p2r.sort_by_layers(w)
+    outs = []
+    for wl in (w, ws):
+        q = p2r.Queue(wl, blocks_per_item=4)
+        t, h = dev(torch, wl["trk"]), dev(torch, wl["hit"])
+        o = torch.empty_like(t)
+        q.run(t, h, o)
+        torch.cuda.synchronize()
+        outs.append(o.cpu().numpy())
+    back = p2r.permute_tracks(outs[1], p2r.inverse(perm), 32, 28)
+    assert np.array_equal(back.view(np.uint32).reshape(-1), outs[0].view(np.uint32).reshape(-1))
 
 
 @pytest.mark.gpu
