@@ -127,7 +127,10 @@ int p2r_count_nonfinite(const void* trk, int64_t nblocks, int32_t bsize, unsigne
  * library-owned pool of three streams so copies overlap kernels (the reference's
  * multi-stream driver, cuda_v4.cu:912-1010). Ordered after prior work on `stream`, and
  * `stream` waits for all of it. Host arrays should be pinned for the copies to overlap.
- * The first call on a device creates the pool (streams and events, no device memory). */
+ * The first call on a device creates the pool (streams and events, no device memory).
+ * Calls from several host threads are serialised while they queue their work (the pool's
+ * streams are shared), and the caller's stream waits for everything queued, also when a step
+ * fails and an error is returned. */
 int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void* host_hits, void* host_trk_out,
                      void* dev_trk_in, void* dev_hits, void* dev_trk_out, int32_t nchunks, void* stream);
 

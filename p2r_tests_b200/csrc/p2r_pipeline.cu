@@ -16,6 +16,7 @@ constexpr int kMaxDevices = 64;
 constexpr int kPoolStreams = 3;
 
 struct StreamPool {
+  std::mutex mu;  // one call at a time enqueues on the pool (the fork / join events are shared)
   bool ready = false;
   cudaStream_t s[kPoolStreams];
   cudaEvent_t fork;
@@ -59,6 +60,7 @@ extern "C" int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, 
   if (cfg->nevts == 0 || cfg->nb == 0) return p2r_clear_error();
   StreamPool* pool = nullptr;
   if ((rc = get_pool(&pool))) return rc;
+  std::lock_guard<std::mutex> lk(pool->mu);
   const int64_t chunks = nchunks > cfg->nevts ? cfg->nevts : nchunks;
   const size_t trk_ev = (size_t)cfg->nb * 28 * cfg->bsize * sizeof(float);
   const size_t hit_ev = (size_t)cfg->nb * cfg->nlayer * 9 * cfg->bsize * sizeof(float);
@@ -66,6 +68,15 @@ extern "C" int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, 
   cudaError_t e = cudaEventRecord(pool->fork, caller);
   for (int i = 0; i < kPoolStreams && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(pool->s[i], pool->fork, 0);
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_host: %s", cudaGetErrorString(e));
+  // the caller's stream waits for everything queued on the pool, also when a step fails
+  auto join = [&]() {
+    cudaError_t je = cudaSuccess;
+    for (int i = 0; i < kPoolStreams && je == cudaSuccess; ++i) {
+      je = cudaEventRecord(pool->join[i], pool->s[i]);
+      if (je == cudaSuccess) je = cudaStreamWaitEvent(caller, pool->join[i], 0);
+    }
+    return je;
+  };
   for (int64_t c = 0; c < chunks; ++c) {
     const int64_t ev0 = cfg->nevts * c / chunks, ev1 = cfg->nevts * (c + 1) / chunks;
     if (ev1 == ev0) continue;
@@ -77,18 +88,23 @@ extern "C" int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, 
                              cudaMemcpyHostToDevice, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync(dh, (const char*)host_hits + ev0 * hit_ev, (ev1 - ev0) * hit_ev,
                              cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    {
+      join();
       return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_host: H2D: %s", cudaGetErrorString(e));
+    }
     p2r_config sub = *cfg;
     sub.nevts = ev1 - ev0;
-    if ((rc = p2r_forward(&sub, dti, dh, dto, nullptr, nullptr, s))) return rc;
+    if ((rc = p2r_forward(&sub, dti, dh, dto, nullptr, nullptr, s))) {
+      join();
+      return rc;
+    }
     if ((e = cudaMemcpyAsync((char*)host_trk_out + ev0 * trk_ev, dto, (ev1 - ev0) * trk_ev, cudaMemcpyDeviceToHost,
-                             s)) != cudaSuccess)
+                             s)) != cudaSuccess) {
+      join();
       return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_host: D2H: %s", cudaGetErrorString(e));
+    }
   }
-  for (int i = 0; i < kPoolStreams && e == cudaSuccess; ++i) {
-    e = cudaEventRecord(pool->join[i], pool->s[i]);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(caller, pool->join[i], 0);
-  }
-  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_host: %s", cudaGetErrorString(e));
+  if ((e = join()) != cudaSuccess)
+    return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_host: %s", cudaGetErrorString(e));
   return p2r_clear_error();
 }

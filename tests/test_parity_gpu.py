@@ -407,3 +407,55 @@ def test_arrays_beyond_32_bit_offsets(p2r, torch):
     torch.cuda.synchronize()
     assert torch.equal(out[-per_t:].view(torch.int32), o1.view(torch.int32))
     del trk, hit, out
+
+
+@pytest.mark.parametrize("nchunks", [1, 3, 10])
+def test_host_buffer_pipeline_equals_device_run(p2r, torch, nchunks):
+    """p2r_forward_host (chunks of events copied in, run and copied out on the library's stream
+    pool) returns exactly the device-resident forward's result, chunk count above the event
+    count included."""
+    cfg, trk, hit = helix(p2r, 5, 6)
+    want = gpu_forward(p2r, torch, cfg, trk, hit)
+    h_t = torch.from_numpy(trk.reshape(-1).copy()).pin_memory()
+    h_h = torch.from_numpy(hit.reshape(-1).copy()).pin_memory()
+    h_o = torch.zeros_like(h_t).pin_memory()
+    d_t, d_h, d_o = torch.empty_like(h_t, device="cuda"), torch.empty_like(h_h, device="cuda"), torch.empty_like(h_t, device="cuda")
+    p2r.forward_host(cfg, h_t.numpy(), h_h.numpy(), h_o.numpy(), d_t, d_h, d_o, nchunks=nchunks)
+    torch.cuda.synchronize()
+    assert np.array_equal(h_o.numpy().view(np.uint32), want.reshape(-1).view(np.uint32))
+
+
+def test_host_buffer_pipeline_from_two_threads(p2r, torch):
+    """Two host threads calling p2r_forward_host at once (each with its own buffers and
+    stream) both get their device-run results."""
+    import threading
+    cases = []
+    for seed in (11, 12):
+        cfg = p2r.Config(bsize=32, nlayer=20, nevts=6, nb=8, bz=3.8)
+        trk, hit = p2r.generate_helix(cfg, p2r.gen_params(bz=3.8, seed=seed))
+        want = gpu_forward(p2r, torch, cfg, trk, hit)
+        h_t = torch.from_numpy(trk.reshape(-1).copy()).pin_memory()
+        h_h = torch.from_numpy(hit.reshape(-1).copy()).pin_memory()
+        h_o = torch.zeros_like(h_t).pin_memory()
+        dev_bufs = (torch.empty_like(h_t, device="cuda"), torch.empty_like(h_h, device="cuda"),
+                    torch.empty_like(h_t, device="cuda"))
+        cases.append((cfg, h_t, h_h, h_o, dev_bufs, torch.cuda.Stream(), want))
+    errors = []
+
+    def work(c):
+        cfg, h_t, h_h, h_o, (d_t, d_h, d_o), s, _ = c
+        try:
+            for _ in range(5):
+                p2r.forward_host(cfg, h_t.numpy(), h_h.numpy(), h_o.numpy(), d_t, d_h, d_o, nchunks=4, stream=s)
+            s.synchronize()
+        except Exception as exc:  # reported below
+            errors.append(exc)
+
+    threads = [threading.Thread(target=work, args=(c,)) for c in cases]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for c in cases:
+        assert np.array_equal(c[3].numpy().view(np.uint32), c[6].reshape(-1).view(np.uint32))
