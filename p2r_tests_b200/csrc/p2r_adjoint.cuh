@@ -104,20 +104,20 @@ P2R_UNROLL
     const T id = r - r0;
     D += id;
     sincos4(id * iptin * kinv, sina, cosa, omc);
-    if (i + 1 != 5) {
-      const T oor0 = (r0 > T(0) && abs_(r - r0) < T(0.0001f)) ? T(1) / r0 : T(0);
-      const T dadipt = id * kinv;
-      const T dadx = -xo * iptin * kinv * oor0;
-      const T dady = -yo * iptin * kinv * oor0;
-      const T pxca = px * cosa, pxsa = px * sina, pyca = py * cosa, pysa = py * sina;
-      T tmp = k * dadx;
-      dDdx -= (xo * (T(1) + tmp * (pxca - pysa)) + yo * tmp * (pyca + pxsa)) * oor0;
-      tmp = k * dady;
-      dDdy -= (xo * tmp * (pxca - pysa) + yo * (T(1) + tmp * (pyca + pxsa))) * oor0;
-      tmp = dadipt * iptin;
-      dDdipt -= k * (xo * (pxca * tmp - pysa * tmp - pyca - pxsa + py) +
-                     yo * (pyca * tmp + pxsa * tmp - pysa + pxca - px)) * pt * oor0;
-      dDdphi += k * (xo * (pysa - px + pxca) - yo * (pxsa - py + pyca)) * oor0;
+    // path derivatives once the step is below 1 um (TBB:714); before that the reference adds
+    // increments scaled by oor0 = 0, which leave the sums unchanged and are skipped here
+    if (i + 1 != 5 && r0 > T(0) && abs_(r - r0) < T(0.0001f)) {
+      const T oor0 = T(1) / r0;
+      // the increments of TBB:716-734 with their shared terms formed once (a1, a2: the
+      // momentum after the step; k*dadx = kn*xo, k*dady = kn*yo since k*kinv = 1)
+      const T a1 = px * cosa - py * sina, a2 = py * cosa + px * sina;
+      const T kn = -iptin * oor0;
+      const T g = (T(1) + kn * (xo * a1 + yo * a2)) * oor0;
+      dDdx -= xo * g;
+      dDdy -= yo * g;
+      const T tt = id * kinv * iptin;  // dadipt * ipt
+      dDdipt -= k * (xo * (a1 * tt - a2 + py) + yo * (a2 * tt + a1 - px)) * pt * oor0;
+      dDdphi += k * (xo * (py * sina + px * cosa - px) - yo * (a2 - py)) * oor0;
     }
     xo = xo + k * (px * sina - py * omc);
     yo = yo + k * (py * sina + px * omc);
