@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--uneven-steps", type=int, default=10)
+    ap.add_argument("--uneven-events", type=int, default=1000, help="events in the uneven-batch workload")
     ap.add_argument("--no-calib", action="store_true", help="skip the 40-layer calibration workload")
     ap.add_argument("--calib-steps", type=int, default=3)
     ap.add_argument("--calib-nevts", type=int, default=100)
@@ -361,12 +362,12 @@ def main():
                 sweep[k] = {"updates_per_s": ups, "ms": t["ms"], "block_threads": t["block_threads"],
                             "stages": t["stages"]}
 
-    # uneven batch: 1000 events, log-normal track counts, 10-25 layers per track, one
+    # uneven batch: 1000 events by default (--uneven-events), log-normal track counts, 10-25 layers per track, one
     # persistent queue launch captured in a CUDA graph, launch shape picked by the autotuner
     uneven = None
     if not args.no_uneven and world == 1:
         from p2r_tests_b200 import autotune
-        counts = p2r.lognormal_counts(1000, median=2000, sigma=1.0, lo=50, hi=20000, seed=7)
+        counts = p2r.lognormal_counts(args.uneven_events, median=2000, sigma=1.0, lo=50, hi=20000, seed=7)
         wl = {bs: p2r.uneven_workload(counts, bsize=bs, nlayer_max=25) for bs in (32, 64)}
         tq = autotune.tune_queue(counts, bsizes=(32, 64), granularity=(1, 4, 16), threads=(64, 128),
                                  stages=(4,), reps=3, use_cache=False, workloads=wl)
@@ -411,7 +412,7 @@ def main():
         same = bool(np.array_equal(back.view(np.uint32).reshape(-1), qref.view(np.uint32).reshape(-1)))
         qs.release()
         del st_, sh_, so_, ws_
-        uneven = {"workload": "1000 events, tracks/event log-normal (median 2000, sigma 1.0) clipped to "
+        uneven = {"workload": f"{args.uneven_events} events, tracks/event log-normal (median 2000, sigma 1.0) clipped to "
                               "[50, 20000], layers/track uniform 10..25, chained",
                   "tracks": int(counts.sum()), "updates": w["updates"], "bsize": tq["bsize"],
                   "blocks_per_item": tq["blocks_per_item"], "block_threads": tq["block_threads"],
