@@ -19,6 +19,7 @@ compiled unmodified into oracle/_ref/) on all host threads, on the same metric a
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import datetime
 import json
 import os
@@ -340,7 +341,29 @@ def main():
             barrier()
             ams = max_over_ranks(a0.elapsed_time(a1)) / args.adj_steps
             adjoint["ckpt_stride"][str(ck)] = {"ms_per_step": ams, "ratio_vs_forward": ams / ms_per_step}
-        del ws
+        # the same kernels instantiated in FP32 (P2R_FLAG_ADJ_FP32): the cost of the structure
+        # without FP64 arithmetic; its gradients do not meet the 1e-3 bar (reported, not the result)
+        cfg32 = dataclasses.replace(cfg, flags=cfg.flags | p2r.FLAG_ADJ_FP32)
+        ws32, fp32 = {}, {}
+        for ck in (1, 5):
+            for _ in range(2):
+                p2r.forward_backward(cfg32, d_trk, d_hit, dr=d_dr, grad_trk_out=g_trk, grad_chi2=g_chi2,
+                                     ckpt_stride=ck, stream=stream, out=ws32)
+            torch.cuda.synchronize()
+            barrier()
+            a0.record(stream)
+            for _ in range(args.adj_steps):
+                p2r.forward_backward(cfg32, d_trk, d_hit, dr=d_dr, grad_trk_out=g_trk, grad_chi2=g_chi2,
+                                     ckpt_stride=ck, stream=stream, out=ws32)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            ams = max_over_ranks(a0.elapsed_time(a1)) / args.adj_steps
+            fp32[str(ck)] = {"ms_per_step": ams, "ratio_vs_forward": ams / ms_per_step}
+        adjoint["fp32_instance"] = {"ckpt_stride": fp32,
+                                    "note": "P2R_FLAG_ADJ_FP32, same tape kernels in float; per-track gradients "
+                                            "~1e-3 at the median, shared Bz gradient ~17 % off: below the 1e-3 bar"}
+        del ws, ws32
         best = min(adjoint["ckpt_stride"], key=lambda k: adjoint["ckpt_stride"][k]["ms_per_step"])
         adjoint["ratio_vs_forward"] = adjoint["ckpt_stride"][best]["ratio_vs_forward"]
         adjoint["best_ckpt_stride"] = int(best)
@@ -517,6 +540,26 @@ def main():
     e2e_ms = max_over_ranks(x0.elapsed_time(x1))
     e2e_value = world * updates * args.e2e_steps / (e2e_ms / 1e3)
     ok = np.array_equal(h_out.view(np.uint32), d_out.cpu().numpy().view(np.uint32))
+    # the link the end-to-end call is bound by: one whole-buffer pinned copy each way, same bytes
+    ht, hh, ho = torch.from_numpy(h_trk), torch.from_numpy(h_hit), torch.from_numpy(h_out)
+    with torch.cuda.stream(stream):
+        c0, c1, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        for rep in range(3):
+            c0.record(stream)
+            d_trk.copy_(ht, non_blocking=True)
+            d_hit.copy_(hh, non_blocking=True)
+            c1.record(stream)
+            ho.copy_(d_out, non_blocking=True)
+            c2.record(stream)
+        torch.cuda.synchronize()
+    h2d_gbs = (trk.nbytes + hit.nbytes) / (c0.elapsed_time(c1) / 1e3) / 1e9
+    d2h_gbs = trk.nbytes / (c1.elapsed_time(c2) / 1e3) / 1e9
+    e2e_s = e2e_ms / 1e3 / args.e2e_steps
+    pcie = {"h2d_gbs_measured": h2d_gbs, "d2h_gbs_measured": d2h_gbs,
+            "achieved_h2d_gbs": (trk.nbytes + hit.nbytes) / e2e_s / 1e9,
+            "frac": (trk.nbytes + hit.nbytes) / e2e_s / 1e9 / h2d_gbs,
+            "how": "one whole-buffer pinned cudaMemcpyAsync per direction (torch copy_), after the "
+                   "end-to-end steps; frac = the end-to-end step's H2D bytes / its time, over h2d_gbs_measured"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -554,7 +597,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "track-layer updates/s",
                     "h2d_bytes_per_step": int(trk.nbytes + hit.nbytes), "d2h_bytes_per_step": int(trk.nbytes),
                     "steps": args.e2e_steps, "api": "p2r_forward_host (pinned host buffers, 10 chunks)",
-                    "output_matches_device_run": bool(ok)},
+                    "output_matches_device_run": bool(ok), "pcie": pcie},
             "fwd_adjoint": adjoint,
             "bsize_sweep": sweep,
             "uneven_batch": uneven,
