@@ -88,8 +88,12 @@ P2R_HD void prop_fwd(const T (&ip)[6], const T (&ic)[21], T k, T kinv, T r, Prop
   t.pt = T(1) / iptin;
   sincos_(phiin, &t.sP, &t.cP);
   T px = t.cP * t.pt, py = t.sP * t.pt;
-  T dDdx = t.r00 > T(0) ? -xin / t.r00 : T(0);
-  T dDdy = t.r00 > T(0) ? -yin / t.r00 : T(0);
+  T dDdx = 0, dDdy = 0;
+  if (t.r00 > T(0)) {
+    const T ir00 = T(1) / t.r00;
+    dDdx = -xin * ir00;
+    dDdy = -yin * ir00;
+  }
   T dDdipt = 0, dDdphi = 0, D = 0, sina, cosa, omc;
   T xo = xin, yo = yin;
   const T pt = t.pt;
@@ -369,8 +373,9 @@ P2R_UNROLL
     pyb = pyb_n;
     T idb = Db;
     T r0b = 0;
+    const T ir0 = r0 > T(0) ? T(1) / r0 : T(0);  // one reciprocal per iteration, used twice
     if (i < 4) {
-      const T o = (r0 > T(0) && abs_(r - r0) < T(0.0001f)) ? T(1) / r0 : T(0);
+      const T o = abs_(r - r0) < T(0.0001f) ? ir0 : T(0);
       if (o != T(0)) {
         const T dxb = -dDdxb, dyb = -dDdyb, dib = -dDdiptb, dpb = dDdphib;  // adjoints of the increments
         const T dadipt_i = id * kinv, dadx_i = -xo * ipt * kinv * o, dady_i = -yo * ipt * kinv * o;
@@ -450,17 +455,15 @@ P2R_UNROLL
     kinvbar += ab * id * ipt;
     rbar += idb;
     r0b -= idb;
-    if (r0 > T(0)) {
-      xob += r0b * xo / r0;
-      yob += r0b * yo / r0;
-    }
+    xob += r0b * xo * ir0;
+    yob += r0b * yo * ir0;
   }
   // ---- initial values: dDdx0 = -x/r00, dDdy0 = -y/r00 (r00 > 0), px0 = cP pt, py0 = sP pt
   if (t.r00 > T(0)) {
-    const T r00 = t.r00;
-    const T r00b = (dDdxb * x + dDdyb * y) / (r00 * r00);
-    xob += -dDdxb / r00 + r00b * x / r00;
-    yob += -dDdyb / r00 + r00b * y / r00;
+    const T ir00 = T(1) / t.r00;
+    const T r00b = (dDdxb * x + dDdyb * y) * ir00 * ir00;
+    xob += (r00b * x - dDdxb) * ir00;
+    yob += (r00b * y - dDdyb) * ir00;
   }
   cPb += pxb * pt;
   sPb += pyb * pt;
@@ -519,7 +522,8 @@ P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T
                     T chi2b, T (&hpb)[3], T (&hcb)[6]) {
   const T rh = hipo(hp[0], hp[1]);
   const T den = T(2) * rh;
-  const T R00 = -(hp[1] + p[1]) / den, R01 = (hp[0] + p[0]) / den;
+  const T iden = T(1) / den;  // one reciprocal for every quotient by den (and by rh = den / 2)
+  const T R00 = -(hp[1] + p[1]) * iden, R01 = (hp[0] + p[0]) * iden;
   T A[6];
 P2R_UNROLL
   for (int k = 0; k < 6; ++k) A[k] = c[k] + hc[k];
@@ -614,14 +618,15 @@ P2R_UNROLL
 P2R_UNROLL
   for (int k = 0; k < 6; ++k) cb[k] += hcb[k];
   // R00 = -(hy + y)/den, R01 = (hx + x)/den, den = 2 hipo(hx, hy)
-  hpb[1] -= R00b / den;
-  pb[1] -= R00b / den;
-  hpb[0] += R01b / den;
-  pb[0] += R01b / den;
-  const T rhb = T(2) * (-(R00b * R00 + R01b * R01) / den);
+  hpb[1] -= R00b * iden;
+  pb[1] -= R00b * iden;
+  hpb[0] += R01b * iden;
+  pb[0] += R01b * iden;
+  const T rhb = T(2) * (-(R00b * R00 + R01b * R01) * iden);
   if (rh > T(0)) {
-    hpb[0] += rhb * hp[0] / rh;
-    hpb[1] += rhb * hp[1] / rh;
+    const T irh = T(2) * iden;
+    hpb[0] += rhb * hp[0] * irh;
+    hpb[1] += rhb * hp[1] * irh;
   }
 }
 
@@ -654,8 +659,9 @@ P2R_UNROLL
   for (int i = 0; i < 21; ++i) cb[i] = cin[i];
   drb += rbar;
   if (rh > T(0)) {
-    hpb[0] += rbar * hp[0] / rh;
-    hpb[1] += rbar * hp[1] / rh;
+    const T irh = T(1) / rh;
+    hpb[0] += rbar * hp[0] * irh;
+    hpb[1] += rbar * hp[1] * irh;
   }
 }
 
