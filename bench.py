@@ -129,9 +129,10 @@ def make_inputs(p2r, nevts, bsize, seed):
     return cfg, trk, hit
 
 
-def traffic_from_profiles(workload_key: str):
-    """Per-launch DRAM bytes of the fused kernel from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / "fwd_kernel_chained_9600x100x20.md"
+def traffic_from_profiles(mode: str):
+    """Per-launch DRAM bytes of the fused kernel (chained or restart) from the committed ncu
+    summary of that mode, if any."""
+    f = ROOT / "profiles" / f"fwd_kernel_{mode}_9600x100x20.md"
     if not f.exists():
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
@@ -224,7 +225,10 @@ def run_reference_arm(args):
 
 
 def workload_config(args):
-    return {"workload": f"fused {args.mode} p2r forward (propagateToR + KalmanUpdate per layer), "
+    what = ("propagateToR + KalmanUpdate per layer" if args.mode == "chained" else
+            "the reference's restart loop: every layer restarts from the input track and rewrites the "
+            "output, so only the last layer is computed, one propagateToR + KalmanUpdate per track")
+    return {"workload": f"fused {args.mode} p2r forward ({what}), "
                         f"{NTRKS} tracks x {args.nevts} events x {NLAYER} layers per GPU",
             "ntrks": NTRKS, "nevts": args.nevts, "nlayer": NLAYER, "bsize": args.bsize, "bz_tesla": BZ,
             "mode": args.mode, "generator": "p2r_gen_helix defaults (seeded synthetic helices)",
@@ -264,7 +268,11 @@ def main():
     d_hit = torch.from_numpy(hit.reshape(-1)).to(dev)
     d_out = torch.empty_like(d_trk)
     stream = torch.cuda.current_stream(dev)
-    updates = cfg.ntracks * NLAYER  # per step per GPU (restart counts the same work unit)
+    # track-layer updates computed per step per GPU. Restart: the reference's restart loop
+    # rewrites the output at every layer from the same input track (TBB:870-926), so only the
+    # last layer reaches the output and only that one is computed: one update per track.
+    restart = cfg.mode == p2r.MODE_RESTART
+    updates = cfg.ntracks * (1 if restart else NLAYER)
 
     def barrier():
         if world > 1:
@@ -319,16 +327,16 @@ def main():
         torch.cuda.synchronize()
         probe_peaks["f32x2" if packed else "f32"] = pflops / (pe0.elapsed_time(pe1) / 1e3) / 1e12
     fp32_peak = max(probe_peaks.values())
-    alg_bytes = cfg.ntracks * (36 * NLAYER + 224)
+    alg_bytes = cfg.ntracks * (36 * (1 if restart else NLAYER) + 224)
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs")
-    traffic = traffic_from_profiles("chained")
+    traffic = traffic_from_profiles(args.mode)
 
     # forward + adjoint (p2r_forward_backward: fused chained forward with checkpoints and
     # the hand-written reverse sweep, plus the deterministic reduction of the shared
     # gradients) against the plain fused forward, on the same workload
     adjoint = None
-    if not args.no_adjoint:
+    if not args.no_adjoint and not restart:  # the adjoint is of the chained loop
         g_trk = torch.randn(d_trk.numel(), dtype=torch.float32, device=dev, generator=torch.Generator(dev).manual_seed(1))
         g_chi2 = torch.ones(cfg.ntracks, dtype=torch.float32, device=dev)
         d_dr = torch.zeros(NLAYER, dtype=torch.float32, device=dev)
@@ -562,16 +570,18 @@ def main():
             c2.record(stream)
         torch.cuda.synchronize()
     h2d_gbs = (trk.nbytes + hit.nbytes) / (c0.elapsed_time(c1) / 1e3) / 1e9
+    # bytes the end-to-end call copies in: restart mode copies only the last layer's hits
+    h2d_step = trk.nbytes + (hit.nbytes // NLAYER if restart else hit.nbytes)
     d2h_gbs = trk.nbytes / (c1.elapsed_time(c2) / 1e3) / 1e9
     e2e_s = e2e_ms / 1e3 / args.e2e_steps
     pcie = {"h2d_gbs_measured": h2d_gbs, "d2h_gbs_measured": d2h_gbs,
-            "achieved_h2d_gbs": (trk.nbytes + hit.nbytes) / e2e_s / 1e9,
-            "frac": (trk.nbytes + hit.nbytes) / e2e_s / 1e9 / h2d_gbs,
+            "achieved_h2d_gbs": h2d_step / e2e_s / 1e9,
+            "frac": h2d_step / e2e_s / 1e9 / h2d_gbs,
             "how": "one whole-buffer pinned cudaMemcpyAsync per direction (torch copy_), after the "
                    "end-to-end steps; frac = the end-to-end step's H2D bytes / its time, over h2d_gbs_measured"}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not restart:  # timed on the chained loop
         try:
             nthreads = len(os.sched_getaffinity(0))
             v, sample, kind, thr = cpu_reference_rate(trk.reshape(-1), hit.reshape(-1), args.nevts, cfg.nb,
@@ -604,7 +614,7 @@ def main():
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                              "algorithmic_bytes_per_launch": alg_bytes},
             "e2e": {"value": e2e_value, "unit": "track-layer updates/s",
-                    "h2d_bytes_per_step": int(trk.nbytes + hit.nbytes), "d2h_bytes_per_step": int(trk.nbytes),
+                    "h2d_bytes_per_step": int(h2d_step), "d2h_bytes_per_step": int(trk.nbytes),
                     "steps": args.e2e_steps, "api": "p2r_forward_host (pinned host buffers, 10 chunks)",
                     "output_matches_device_run": bool(ok), "pcie": pcie},
             "fwd_adjoint": adjoint,

@@ -130,7 +130,9 @@ int p2r_count_nonfinite(const void* trk, int64_t nblocks, int32_t bsize, unsigne
  * The first call on a device creates the pool (streams and events, no device memory).
  * Calls from several host threads are serialised while they queue their work (the pool's
  * streams are shared), and the caller's stream waits for everything queued, also when a step
- * fails and an error is returned. */
+ * fails and an error is returned. In restart mode only the last layer's hit blocks are copied
+ * (the only layer whose result reaches the output); the other layers' part of dev_hits is left
+ * as it was. */
 int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void* host_hits, void* host_trk_out,
                      void* dev_trk_in, void* dev_hits, void* dev_trk_out, int32_t nchunks, void* stream);
 

@@ -4,6 +4,9 @@
 // driver (cuda_v4.cu:912-1010: per-stream cudaMemcpyAsync H2D, kernel, D2H), over the same
 // Matriplex arrays. Events are contiguous in both arrays (track block ib + nb*ev, hit block
 // lay + nlayer*(ib + nb*ev)), so a chunk of events is one contiguous byte range of each.
+// In restart mode only the last layer reaches the output (the reference's restart loop
+// rewrites it at every layer from the same input track), so only that layer's hit block of
+// each track block is copied: one strided 2-D copy per chunk, a 1/nlayer share of the hits.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -64,6 +67,9 @@ extern "C" int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, 
   const int64_t chunks = nchunks > cfg->nevts ? cfg->nevts : nchunks;
   const size_t trk_ev = (size_t)cfg->nb * 28 * cfg->bsize * sizeof(float);
   const size_t hit_ev = (size_t)cfg->nb * cfg->nlayer * 9 * cfg->bsize * sizeof(float);
+  const size_t hit_blk = (size_t)9 * cfg->bsize * sizeof(float);  // one layer of one track block
+  const size_t last = (size_t)(cfg->nlayer - 1) * hit_blk;          // offset of the last layer's block
+  const bool restart = cfg->mode == P2R_MODE_RESTART;
   cudaStream_t caller = (cudaStream_t)stream;
   cudaError_t e = cudaEventRecord(pool->fork, caller);
   for (int i = 0; i < kPoolStreams && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(pool->s[i], pool->fork, 0);
@@ -86,8 +92,11 @@ extern "C" int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, 
     char* dto = (char*)dev_trk_out + ev0 * trk_ev;
     if ((e = cudaMemcpyAsync(dti, (const char*)host_trk_in + ev0 * trk_ev, (ev1 - ev0) * trk_ev,
                              cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(dh, (const char*)host_hits + ev0 * hit_ev, (ev1 - ev0) * hit_ev,
-                             cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        (e = restart ? cudaMemcpy2DAsync(dh + last, (size_t)cfg->nlayer * hit_blk,
+                                         (const char*)host_hits + ev0 * hit_ev + last, (size_t)cfg->nlayer * hit_blk,
+                                         hit_blk, (size_t)(ev1 - ev0) * cfg->nb, cudaMemcpyHostToDevice, s)
+                     : cudaMemcpyAsync(dh, (const char*)host_hits + ev0 * hit_ev, (ev1 - ev0) * hit_ev,
+                                       cudaMemcpyHostToDevice, s)) != cudaSuccess)
     {
       join();
       return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_host: H2D: %s", cudaGetErrorString(e));

@@ -409,20 +409,25 @@ def test_arrays_beyond_32_bit_offsets(p2r, torch):
     del trk, hit, out
 
 
+@pytest.mark.parametrize("mode", ["chained", "restart"])
 @pytest.mark.parametrize("nchunks", [1, 3, 10])
-def test_host_buffer_pipeline_equals_device_run(p2r, torch, nchunks):
+def test_host_buffer_pipeline_equals_device_run(p2r, torch, nchunks, mode):
     """p2r_forward_host (chunks of events copied in, run and copied out on the library's stream
     pool) returns exactly the device-resident forward's result, chunk count above the event
-    count included."""
+    count included; in restart mode it copies only the last layer's hits (a strided copy)."""
     cfg, trk, hit = helix(p2r, 5, 6)
+    cfg.mode = MODES[mode]
     want = gpu_forward(p2r, torch, cfg, trk, hit)
     h_t = torch.from_numpy(trk.reshape(-1).copy()).pin_memory()
     h_h = torch.from_numpy(hit.reshape(-1).copy()).pin_memory()
     h_o = torch.zeros_like(h_t).pin_memory()
     d_t, d_h, d_o = torch.empty_like(h_t, device="cuda"), torch.empty_like(h_h, device="cuda"), torch.empty_like(h_t, device="cuda")
+    d_h.fill_(float("nan"))  # restart: layers that are not copied must not be read either
     p2r.forward_host(cfg, h_t.numpy(), h_h.numpy(), h_o.numpy(), d_t, d_h, d_o, nchunks=nchunks)
     torch.cuda.synchronize()
     assert np.array_equal(h_o.numpy().view(np.uint32), want.reshape(-1).view(np.uint32))
+    copied = np.isfinite(d_h.cpu().numpy().reshape(cfg.nblocks, cfg.nlayer, -1)).all(2)
+    assert copied[:, -1].all() and (copied[:, :-1].all() if mode == "chained" else not copied[:, :-1].any())
 
 
 def test_host_buffer_pipeline_from_two_threads(p2r, torch):
