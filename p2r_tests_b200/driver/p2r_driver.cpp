@@ -213,7 +213,8 @@ int main(int argc, char** argv) {
   std::printf("done ntracks=%ld tot time=%f (s) time/trk=%e (s)\n", ntracks, wall_time, wall_time / ntracks);
   std::printf("formatted %d %ld %ld %d %ld %f 0 %f %d\n", a.niter, a.nevts, a.ntrks, a.bsize, nb, wall_time, setup_time,
               1);
-  std::printf("track-layer updates/s=%e\n", (double)ntracks * a.nlayer / wall_time);
+  // restart: only the last layer reaches the output and only that one is computed
+  std::printf("track-layer updates/s=%e\n", (double)ntracks * (a.chained ? a.nlayer : 1) / wall_time);
 
   if (!a.transfer) CU(cudaMemcpy(out.data(), d_out, trk_words * 4, cudaMemcpyDeviceToHost));
   p2r_summary_stats s;
