@@ -506,14 +506,19 @@ def main():
         del o4, t4s, h4s, nl4s
         gc4 = torch.ones(c4.ntracks, dtype=torch.float32, device=dev)
         out4 = {"grad_trk_in": None, "grad_hits": None}
+        # checkpoint stride: 1 (the whole state tape, the fastest reverse) when its workspace fits
+        # in 70 % of the free device memory, else 5
+        torch.cuda.empty_cache()
+        free4, _ = torch.cuda.mem_get_info(dev)
+        ck4 = 1 if p2r.workspace_size(c4, 1) <= 0.7 * free4 else 5
         p2r.forward_backward(c4, t4, h4, dr=dr4, nlay_lane=nl4, grad_chi2=gc4, per_event=True, out=out4,
-                             stream=stream)
+                             ckpt_stride=ck4, stream=stream)
         torch.cuda.synchronize()
         graph4 = torch.cuda.CUDAGraph()
         cap = torch.cuda.Stream(device=dev)  # capture needs a non-default stream; replays run on the current one
         with torch.cuda.graph(graph4, stream=cap):
             p2r.forward_backward(c4, t4, h4, dr=dr4, nlay_lane=nl4, grad_chi2=gc4, per_event=True, out=out4,
-                                 stream=cap)
+                                 ckpt_stride=ck4, stream=cap)
         graph4.replay()
         torch.cuda.synchronize()
         b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -532,8 +537,9 @@ def main():
                              "api": "p2r_forward_masked (fused, per-track layer counts)",
                              "sorted_by_layer_count": {"ms_per_step": fms_sorted,
                                                        "updates_per_s": upd4 / (fms_sorted / 1e3)}},
-                 "forward_adjoint": {"ms_per_step": bms, "ratio_vs_forward": bms / fms,
-                                     "api": "p2r_forward_backward (FP64, ckpt 5), per-event grad_dr/grad_bz, "
+                 "forward_adjoint": {"ms_per_step": bms, "ratio_vs_forward": bms / fms, "ckpt_stride": ck4,
+                                     "workspace_bytes": p2r.workspace_size(c4, ck4),
+                                     "api": f"p2r_forward_backward (FP64, ckpt {ck4}), per-event grad_dr/grad_bz, "
                                             "replayed from one CUDA graph"},
                  "per_event_sum_matches_total": bool(torch.allclose(ev_sum, out4["grad_dr"], rtol=1e-10, atol=0)),
                  "steps": args.calib_steps}

@@ -134,17 +134,24 @@ def tune_queue(ntrk_event, bsizes=(32, 64, 128), granularity=(1, 2, 4, 8, 16), t
     return out
 
 
-def tune_adjoint(cfg: Config, d_trk, d_hit, strides=(1, 2, 4, 5, 10), reps: int = 3, use_cache: bool = True) -> dict:
-    """Best checkpoint stride for p2r_forward_backward on device arrays d_trk / d_hit."""
+def tune_adjoint(cfg: Config, d_trk, d_hit, strides=(1, 2, 4, 5, 10), reps: int = 3, use_cache: bool = True,
+                 max_workspace_bytes: int | None = None) -> dict:
+    """Best checkpoint stride for p2r_forward_backward on device arrays d_trk / d_hit.
+    A smaller stride keeps more of the state on the tape (faster reverse, larger workspace:
+    27 values per track per checkpoint); strides whose workspace exceeds max_workspace_bytes
+    are not tried (None: no limit)."""
     import torch
 
-    from .autograd import forward_backward
-    key = (f"{_gpu_name()}|adjoint|ntr={cfg.ntracks}|nlayer={cfg.nlayer}|flags={cfg.flags}")
+    from .autograd import forward_backward, workspace_size
+    fits = [ck for ck in strides if max_workspace_bytes is None or workspace_size(cfg, ck) <= max_workspace_bytes]
+    if not fits:
+        raise ValueError(f"no checkpoint stride in {tuple(strides)} fits {max_workspace_bytes} bytes of workspace")
+    key = (f"{_gpu_name()}|adjoint|ntr={cfg.ntracks}|nlayer={cfg.nlayer}|flags={cfg.flags}|strides={fits}")
     if use_cache and key in _load_cache():
         return _load_cache()[key]
     g_chi2 = torch.ones(cfg.ntracks, dtype=torch.float32, device=d_trk.device)
     results, ws = [], {}
-    for ck in strides:
+    for ck in fits:
         forward_backward(cfg, d_trk, d_hit, grad_chi2=g_chi2, ckpt_stride=ck, out=ws)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()

@@ -159,3 +159,11 @@ def test_tune_adjoint_picks_a_timed_stride(p2r, torch, helix, tmp_path, monkeypa
     t = autotune.tune_adjoint(cfg, d_trk, d_hit, strides=(1, 5, 10), reps=1, use_cache=False)
     assert [x["ckpt_stride"] for x in t["tried"]] == [1, 5, 10]
     assert t["ckpt_stride"] in (1, 5, 10) and t["ms"] == min(x["ms"] for x in t["tried"])
+    # a workspace budget below the stride-1 tape leaves only the larger strides
+    budget = max(p2r.workspace_size(cfg, 5), p2r.workspace_size(cfg, 10))  # 10 keeps a 9-slot segment buffer
+    assert p2r.workspace_size(cfg, 1) > budget
+    t = autotune.tune_adjoint(cfg, d_trk, d_hit, strides=(1, 5, 10), reps=1, use_cache=False,
+                              max_workspace_bytes=budget)
+    assert [x["ckpt_stride"] for x in t["tried"]] == [5, 10]
+    with pytest.raises(ValueError):
+        autotune.tune_adjoint(cfg, d_trk, d_hit, strides=(1,), reps=1, use_cache=False, max_workspace_bytes=budget)
