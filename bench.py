@@ -139,6 +139,16 @@ def traffic_from_profiles(mode: str):
     return float(m.group(1)) if m else None
 
 
+def fp64_flop_per_update():
+    """Executed FP64 FLOPs per track-layer of the stride-1 FP64 adjoint (forward with tape +
+    reverse), from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / "tape_adjoint_fp64_ck1_9600x8x20.md"
+    if not f.exists():
+        return None
+    m = re.search(r"fp64_flop_per_update:\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
 def measured_peaks():
     f = ROOT / "MEASURED_PEAKS.json"
     try:
@@ -327,6 +337,17 @@ def main():
         torch.cuda.synchronize()
         probe_peaks["f32x2" if packed else "f32"] = pflops / (pe0.elapsed_time(pe1) / 1e3) / 1e12
     fp32_peak = max(probe_peaks.values())
+    # the FP64 FMA peak: the denominator of the FP64 adjoint's roofline
+    probe64 = torch.empty(148 * 8 * 256, dtype=torch.float64, device=dev)
+    p2r.fp64_fma_probe(probe64, 200, 148 * 8, 256, stream=stream)
+    torch.cuda.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record(stream)
+    pflops = sum(p2r.fp64_fma_probe(probe64, 2000, 148 * 8, 256, stream=stream) for _ in range(5))
+    pe1.record(stream)
+    torch.cuda.synchronize()
+    fp64_peak = pflops / (pe0.elapsed_time(pe1) / 1e3) / 1e12
+    del probe64
     alg_bytes = cfg.ntracks * (36 * (1 if restart else NLAYER) + 224)
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs")
@@ -383,6 +404,15 @@ def main():
         del ws, ws32
         best = min(adjoint["ckpt_stride"], key=lambda k: adjoint["ckpt_stride"][k]["ms_per_step"])
         adjoint["ratio_vs_forward"] = adjoint["ckpt_stride"][best]["ratio_vs_forward"]
+        f64u = fp64_flop_per_update()
+        if f64u and best == "1":  # the executed FP64 work is counted for the stride-1 tape kernels
+            a64 = f64u * updates / (adjoint["ckpt_stride"]["1"]["ms_per_step"] / 1e3) / 1e12
+            adjoint["roofline_fp64"] = {
+                "bound": "fp64", "achieved": a64, "peak": fp64_peak, "unit": "TFLOP/s", "frac": a64 / fp64_peak,
+                "fp64_flop_per_update": f64u,
+                "peak_source": "measured in this run: p2r_fp64_fma_probe (DFMA), full occupancy",
+                "flop_source": "executed DADD + DMUL + 2 DFMA per track-layer of fwd_tape_kernel + "
+                               "rev_tape_kernel<double, 1>, ncu counters (profiles/tape_adjoint_fp64_ck1_9600x8x20.md)"}
         adjoint["best_ckpt_stride"] = int(best)
         adjoint["definition"] = ("time of p2r_forward_backward in FP64 (forward outputs + gradients w.r.t. initial "
                                  "parameters/covariance, hits, per-layer dr and Bz of sum(g.out) + sum(chi2)), "

@@ -267,6 +267,9 @@ int p2r_autotune_forward(const p2r_config* cfg, const void* trk_in, const void* 
 int p2r_fp32_fma_probe(int64_t iters, int32_t blocks, int32_t threads, float* out, void* stream);
 /* The same probe with packed f32x2 FMAs (sm_100's two-lane form); same FLOPs per launch. */
 int p2r_fp32x2_fma_probe(int64_t iters, int32_t blocks, int32_t threads, float* out, void* stream);
+/* The same probe in FP64 (the denominator of the FP64 adjoint's roofline); same FLOPs per
+ * launch, out: blocks*threads doubles. */
+int p2r_fp64_fma_probe(int64_t iters, int32_t blocks, int32_t threads, double* out, void* stream);
 
 /* The division / square-root build of the hot path (no reference counterpart; the reference
  * takes whatever its compiler flags give). P2R_MATH_REFINED: hardware reciprocal and

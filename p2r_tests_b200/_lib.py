@@ -113,6 +113,7 @@ SIGNATURES = {
     "p2r_forward_host": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "p2r_fp32_fma_probe": (ctypes.c_int, [_i64, _i32, _i32, _vp, _vp]),
     "p2r_fp32x2_fma_probe": (ctypes.c_int, [_i64, _i32, _i32, _vp, _vp]),
+    "p2r_fp64_fma_probe": (ctypes.c_int, [_i64, _i32, _i32, _vp, _vp]),
     "p2r_math_variant": (ctypes.c_int32, []),
     "p2r_math_check": (ctypes.c_int, [_i64, _vp, _vp, _vp, _vp, _vp]),
     "p2r_forward_backward_workspace_size": (ctypes.c_size_t, [_cfgp]),

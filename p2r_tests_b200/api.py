@@ -154,6 +154,12 @@ def fp32_fma_probe(out, iters: int, blocks: int, threads: int = 256, stream=None
     return 64 * iters * blocks * threads
 
 
+def fp64_fma_probe(out, iters: int, blocks: int, threads: int = 256, stream=None) -> int:
+    """Launches the FP64 FMA probe (out: float64, blocks*threads); returns the FLOPs it performs."""
+    check(lib().p2r_fp64_fma_probe(iters, blocks, threads, _ptr(out), _stream(stream)))
+    return 64 * iters * blocks * threads
+
+
 def math_variant() -> str:
     """Which division / square-root build the library is: "refined", "ieee" or "fast"."""
     return {_lib.MATH_REFINED: "refined", _lib.MATH_IEEE: "ieee", _lib.MATH_FAST: "fast"}[lib().p2r_math_variant()]

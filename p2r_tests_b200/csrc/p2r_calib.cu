@@ -58,6 +58,28 @@ __global__ void __launch_bounds__(256) fma2_probe_kernel(long long iters, float*
   out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// FP64 FMA throughput probe (the denominator of the FP64 adjoint's compute roofline): the FP32
+// probe's structure in double, 8 independent chains x 4 unrolled rounds per iteration.
+__global__ void __launch_bounds__(256) dfma_probe_kernel(long long iters, double* out) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+  double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+  const double m = 0.999999999, c = 1e-9;
+  for (long long i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a0 = fma(a0, m, c);
+      a1 = fma(a1, m, c);
+      a2 = fma(a2, m, c);
+      a3 = fma(a3, m, c);
+      a4 = fma(a4, m, c);
+      a5 = fma(a5, m, c);
+      a6 = fma(a6, m, c);
+      a7 = fma(a7, m, c);
+    }
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+}
+
 // The hot path's own division and square root (p2r::fdiv, p2r::fsqrt) over caller arrays,
 // so their error against the correctly rounded results can be measured.
 __global__ void math_check_kernel(long long n, const float* __restrict__ a, const float* __restrict__ b,
@@ -107,5 +129,15 @@ extern "C" int p2r_fp32_fma_probe(int64_t iters, int32_t blocks, int32_t threads
   fma_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_fp32_fma_probe: %s", cudaGetErrorString(e));
+  return p2r_clear_error();
+}
+
+// FLOPs per launch = 2 * 32 * iters * blocks * threads, in FP64.
+extern "C" int p2r_fp64_fma_probe(int64_t iters, int32_t blocks, int32_t threads, double* out, void* stream) {
+  if (!out || iters < 1 || blocks < 1 || threads < 32 || threads > 256 || threads % 32)
+    return p2r_set_error(P2R_ERR_INVALID, "p2r_fp64_fma_probe: bad arguments");
+  dfma_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_fp64_fma_probe: %s", cudaGetErrorString(e));
   return p2r_clear_error();
 }
