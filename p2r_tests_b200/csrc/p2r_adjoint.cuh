@@ -263,55 +263,42 @@ P2R_UNROLL
   // ---- Jacobian entries -> their inputs
   const T U = cP * ca - sP * sa, V = sP * ca + cP * sa, w = ipt * dadipt;
   T Ub = 0, Vb = 0, wb = 0, dadxb = 0, dadyb = 0, dadiptb = 0, dadphib = 0, cPb = 0, sPb = 0;
-  kbar += J00b * dadx * U * pt;
-  dadxb += J00b * k * U * pt;
-  Ub += J00b * k * dadx * pt;
-  ptb += J00b * k * dadx * U;
-  kbar += J01b * dady * U * pt;
-  dadyb += J01b * k * U * pt;
-  Ub += J01b * k * dady * pt;
-  ptb += J01b * k * dady * U;
+  const T kp = k * pt;
   {
-    const T Q = w * U - V + sP, g = J03b * k * pt * pt;
-    kbar += J03b * pt * pt * Q;
-    ptb += J03b * T(2) * k * pt * Q;
-    wb += g * U;
-    Ub += g * w;
-    Vb -= g;
-    sPb += g;
+    // J00 = 1 + k dadx U pt, J01 = k dady U pt, J10 = k dadx V pt, J11 = 1 + k dady V pt
+    const T a = J00b * dadx + J01b * dady, b = J10b * dadx + J11b * dady;
+    const T e = a * U + b * V;
+    kbar += e * pt;
+    ptb += e * k;
+    Ub += a * kp;
+    Vb += b * kp;
+    dadxb += (J00b * U + J10b * V) * kp;
+    dadyb += (J01b * U + J11b * V) * kp;
   }
   {
-    const T Q = (dadphi + T(1)) * U - cP, g = J04b * k * pt;
-    kbar += J04b * pt * Q;
-    ptb += J04b * k * Q;
-    dadphib += g * U;
-    Ub += g * (dadphi + T(1));
-    cPb -= g;
-  }
-  kbar += J10b * dadx * V * pt;
-  dadxb += J10b * k * V * pt;
-  Vb += J10b * k * dadx * pt;
-  ptb += J10b * k * dadx * V;
-  kbar += J11b * dady * V * pt;
-  dadyb += J11b * k * V * pt;
-  Vb += J11b * k * dady * pt;
-  ptb += J11b * k * dady * V;
-  {
-    const T Q = w * V + U - cP, g = J13b * k * pt * pt;
-    kbar += J13b * pt * pt * Q;
-    ptb += J13b * T(2) * k * pt * Q;
-    wb += g * V;
-    Vb += g * w;
-    Ub += g;
-    cPb -= g;
+    // J03 = k Q3 pt^2, Q3 = w U - V + sP;  J13 = k Q13 pt^2, Q13 = w V + U - cP
+    const T e = J03b * (w * U - V + sP) + J13b * (w * V + U - cP);
+    kbar += e * pt * pt;
+    ptb += T(2) * e * kp;
+    const T g3 = J03b * kp * pt, g13 = J13b * kp * pt;
+    wb += g3 * U + g13 * V;
+    Ub += g3 * w + g13;
+    Vb += g13 * w - g3;
+    sPb += g3;
+    cPb -= g13;
   }
   {
-    const T Q = (dadphi + T(1)) * V - sP, g = J14b * k * pt;
-    kbar += J14b * pt * Q;
-    ptb += J14b * k * Q;
-    dadphib += g * V;
-    Vb += g * (dadphi + T(1));
-    sPb -= g;
+    // J04 = k Q4 pt, Q4 = (dadphi + 1) U - cP;  J14 = k Q14 pt, Q14 = (dadphi + 1) V - sP
+    const T d1 = dadphi + T(1);
+    const T e = J04b * (d1 * U - cP) + J14b * (d1 * V - sP);
+    kbar += e * pt;
+    ptb += e * k;
+    const T g4 = J04b * kp, g14 = J14b * kp;
+    dadphib += g4 * U + g14 * V;
+    Ub += g4 * d1;
+    Vb += g14 * d1;
+    cPb -= g4;
+    sPb -= g14;
   }
   {
     const T G = k * cT * pt * isT;
@@ -377,75 +364,66 @@ P2R_UNROLL
     if (i < 4) {
       const T o = abs_(r - r0) < T(0.0001f) ? ir0 : T(0);
       if (o != T(0)) {
-        const T dxb = -dDdxb, dyb = -dDdyb, dib = -dDdiptb, dpb = dDdphib;  // adjoints of the increments
-        const T dadipt_i = id * kinv, dadx_i = -xo * ipt * kinv * o, dady_i = -yo * ipt * kinv * o;
-        const T pxca = px * cai, pxsa = px * sai, pyca = py * cai, pysa = py * sai;
-        const T m1 = pxca - pysa, m2 = pyca + pxsa;
-        const T t1 = k * dadx_i, t2 = k * dady_i, t3 = dadipt_i * ipt;
-        T ob = 0, m1b = 0, m2b = 0;
-        // inc_x = (xo (1 + t1 m1) + yo t1 m2) o
-        xob += dxb * (T(1) + t1 * m1) * o;
-        yob += dxb * t1 * m2 * o;
-        const T t1b = dxb * (xo * m1 + yo * m2) * o;
-        m1b += dxb * xo * t1 * o;
-        m2b += dxb * yo * t1 * o;
-        ob += dxb * (xo * (T(1) + t1 * m1) + yo * t1 * m2);
-        // inc_y = (xo t2 m1 + yo (1 + t2 m2)) o
-        xob += dyb * t2 * m1 * o;
-        yob += dyb * (T(1) + t2 * m2) * o;
-        const T t2b = dyb * (xo * m1 + yo * m2) * o;
-        m1b += dyb * xo * t2 * o;
-        m2b += dyb * yo * t2 * o;
-        ob += dyb * (xo * t2 * m1 + yo * (T(1) + t2 * m2));
-        // inc_ipt = k Q pt o, Q = xo (m1 t3 - m2 + py) + yo (m2 t3 + m1 - px)
-        const T Q = xo * (m1 * t3 - m2 + py) + yo * (m2 * t3 + m1 - px);
-        kbar += dib * Q * pt * o;
-        ptb += dib * k * Q * o;
-        ob += dib * k * Q * pt;
-        const T Qb = dib * k * pt * o;
-        xob += Qb * (m1 * t3 - m2 + py);
-        yob += Qb * (m2 * t3 + m1 - px);
-        m1b += Qb * (xo * t3 + yo);
-        m2b += Qb * (-xo + yo * t3);
-        const T t3b = Qb * (xo * m1 + yo * m2);
-        pyb += Qb * xo;
-        pxb -= Qb * yo;
-        // inc_phi = k P o, P = xo n1 - yo n2, n1 = py sa + px ca - px, n2 = px sa + py ca - py
-        const T n1 = pysa + pxca - px, n2 = pxsa + pyca - py;
-        const T P = xo * n1 - yo * n2;
-        kbar += dpb * P * o;
-        ob += dpb * k * P;
-        const T Pb = dpb * k * o;
-        xob += Pb * n1;
-        yob -= Pb * n2;
-        const T n1b = Pb * xo, n2b = -Pb * yo;
-        pyb += n1b * sai;
-        sab_i += n1b * py;
-        pxb += n1b * (cai - T(1));
-        cab_i += n1b * px;
-        pxb += n2b * sai;
-        sab_i += n2b * px;
-        pyb += n2b * (cai - T(1));
-        cab_i += n2b * py;
-        // m1 = px ca - py sa, m2 = py ca + px sa
-        pxb += m1b * cai + m2b * sai;
-        pyb += -m1b * sai + m2b * cai;
-        cab_i += m1b * px + m2b * py;
-        sab_i += -m1b * py + m2b * px;
-        // t1 = k dadx_i, t2 = k dady_i, t3 = dadipt_i ipt
-        kbar += t1b * dadx_i + t2b * dady_i;
-        const T dadxib = t1b * k, dadyib = t2b * k, dadiptib = t3b * ipt;
-        iptb += t3b * dadipt_i;
-        xob -= dadxib * ipt * kinv * o;
-        iptb -= dadxib * xo * kinv * o;
-        kinvbar -= dadxib * xo * ipt * o;
-        ob -= dadxib * xo * ipt * kinv;
-        yob -= dadyib * ipt * kinv * o;
-        iptb -= dadyib * yo * kinv * o;
-        kinvbar -= dadyib * yo * ipt * o;
-        ob -= dadyib * yo * ipt * kinv;
-        idb += dadiptib * kinv;
-        kinvbar += dadiptib * id;
+        // Reverse of the increments in prop_fwd's factored form: with a1, a2 the momentum
+        // after the step, s = xo a1 + yo a2, kn = -ipt o, g = (1 + kn s) o, tt = id kinv ipt:
+        //   dDdx -= xo g,  dDdy -= yo g,
+        //   dDdipt -= k E pt o,  E = xo (a1 tt - a2 + py) + yo (a2 tt + a1 - px),
+        //   dDdphi += k F o,     F = xo (py sa + px ca - px) - yo (a2 - py).
+        const T ca = cai, sa = sai;
+        const T a1 = px * ca - py * sa, a2 = py * ca + px * sa;
+        const T sxy = xo * a1 + yo * a2;
+        const T kn = -ipt * o;
+        const T g = (T(1) + kn * sxy) * o;
+        const T tt = id * kinv * ipt;
+        const T ex = a1 * tt - a2 + py, ey = a2 * tt + a1 - px;
+        const T E = xo * ex + yo * ey;
+        const T fx = py * sa + px * ca - px, fy = a2 - py;
+        const T F = xo * fx - yo * fy;
+        T ob = 0, a1b = 0, a2b = 0;
+        // dDdx, dDdy
+        const T gb = -(dDdxb * xo + dDdyb * yo);
+        xob -= dDdxb * g;
+        yob -= dDdyb * g;
+        ob += gb * (T(1) + kn * sxy);
+        const T knb = gb * o * sxy, sb = gb * o * kn;
+        iptb -= knb * o;
+        ob -= knb * ipt;
+        xob += sb * a1;
+        yob += sb * a2;
+        a1b += sb * xo;
+        a2b += sb * yo;
+        // dDdipt
+        const T Tb = -dDdiptb;
+        kbar += Tb * E * pt * o;
+        ptb += Tb * k * E * o;
+        ob += Tb * k * E * pt;
+        const T Eb = Tb * k * pt * o;
+        xob += Eb * ex;
+        yob += Eb * ey;
+        a1b += Eb * (xo * tt + yo);
+        a2b += Eb * (yo * tt - xo);
+        pyb += Eb * xo;
+        pxb -= Eb * yo;
+        const T ttb = Eb * sxy;
+        idb += ttb * kinv * ipt;
+        kinvbar += ttb * id * ipt;
+        iptb += ttb * id * kinv;
+        // dDdphi
+        kbar += dDdphib * F * o;
+        ob += dDdphib * k * F;
+        const T Fb = dDdphib * k * o;
+        xob += Fb * fx;
+        yob -= Fb * fy;
+        pyb += Fb * (xo * sa + yo);
+        pxb += Fb * xo * (ca - T(1));
+        sab_i += Fb * xo * py;
+        cab_i += Fb * xo * px;
+        a2b -= Fb * yo;
+        // a1 = px ca - py sa, a2 = py ca + px sa
+        pxb += a1b * ca + a2b * sa;
+        pyb += a2b * ca - a1b * sa;
+        cab_i += a1b * px + a2b * py;
+        sab_i += a2b * px - a1b * py;
         r0b -= ob * o * o;
       }
     }
