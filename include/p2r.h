@@ -19,7 +19,10 @@
  * Conventions: every pointer is a device pointer unless its name starts with host_;
  * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream); calls are
  * asynchronous and stream-ordered; nothing allocates device memory except where a
- * function says so. Every function returns a p2r_status; p2r_last_error_string() gives
+ * function says so. Device arrays must be aligned to their element size (4 bytes for the
+ * float / int32 arrays, 8 for double and 64-bit ones; the hit array of the persistent queue to
+ * 16): a misaligned pointer is rejected with P2R_ERR_INVALID before anything is launched.
+ * Every function returns a p2r_status; p2r_last_error_string() gives
  * the message of the calling thread's last failure. No function aborts the process
  * (the reference aborts on CUDA errors, include/cudaCheck.h:17-58).
  */

@@ -550,6 +550,10 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   const long long nblocks = (long long)cfg->nevts * cfg->nb;
   if (nblocks == 0) return p2r_clear_error();
   if (!trk_in || !hits) return p2r_set_errorf(P2R_ERR_INVALID, "%s: null input array", who);
+  if ((rc = p2r_check_aligned(who, 4, {trk_in, hits, dr, nlay_lane, trk_out, chi2_out, grad_trk_out, grad_chi2,
+                                       grad_trk_in, grad_hits})) ||
+      (rc = p2r_check_aligned(who, 8, {grad_dr, grad_bz, grad_dr_event, grad_bz_event})))
+    return rc;
   if ((grad_dr_event || grad_bz_event) && cfg->bsize % 32 != 0)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: per-event gradients need bsize %% 32 == 0", who);
   const WsLayout w = layout_of(cfg);

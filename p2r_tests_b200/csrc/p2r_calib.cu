@@ -95,6 +95,7 @@ __global__ void math_check_kernel(long long n, const float* __restrict__ a, cons
 extern "C" int p2r_fp32x2_fma_probe(int64_t iters, int32_t blocks, int32_t threads, float* out, void* stream) {
   if (!out || iters < 1 || blocks < 1 || threads < 32 || threads > 256 || threads % 32)
     return p2r_set_error(P2R_ERR_INVALID, "p2r_fp32x2_fma_probe: bad arguments");
+  if (int rc = p2r_check_aligned("p2r_fp32x2_fma_probe", 4, {out})) return rc;
   fma2_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_fp32x2_fma_probe: %s", cudaGetErrorString(e));
@@ -114,6 +115,7 @@ extern "C" int32_t p2r_math_variant(void) {
 extern "C" int p2r_math_check(int64_t n, const float* a, const float* b, float* quot, float* root, void* stream) {
   if (n < 0 || (n > 0 && (!a || !b || !quot || !root)))
     return p2r_set_error(P2R_ERR_INVALID, "p2r_math_check: bad arguments");
+  if (int rc = p2r_check_aligned("p2r_math_check", 4, {a, b, quot, root})) return rc;
   if (n == 0) return p2r_clear_error();
   const long long blocks = (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16;
   math_check_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(n, a, b, quot, root);
@@ -126,6 +128,7 @@ extern "C" int p2r_math_check(int64_t n, const float* a, const float* b, float* 
 extern "C" int p2r_fp32_fma_probe(int64_t iters, int32_t blocks, int32_t threads, float* out, void* stream) {
   if (!out || iters < 1 || blocks < 1 || threads < 32 || threads > 256 || threads % 32)
     return p2r_set_error(P2R_ERR_INVALID, "p2r_fp32_fma_probe: bad arguments");
+  if (int rc = p2r_check_aligned("p2r_fp32_fma_probe", 4, {out})) return rc;
   fma_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_fp32_fma_probe: %s", cudaGetErrorString(e));
@@ -136,6 +139,7 @@ extern "C" int p2r_fp32_fma_probe(int64_t iters, int32_t blocks, int32_t threads
 extern "C" int p2r_fp64_fma_probe(int64_t iters, int32_t blocks, int32_t threads, double* out, void* stream) {
   if (!out || iters < 1 || blocks < 1 || threads < 32 || threads > 256 || threads % 32)
     return p2r_set_error(P2R_ERR_INVALID, "p2r_fp64_fma_probe: bad arguments");
+  if (int rc = p2r_check_aligned("p2r_fp64_fma_probe", 8, {out})) return rc;
   dfma_probe_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(iters, out);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_fp64_fma_probe: %s", cudaGetErrorString(e));

@@ -35,6 +35,16 @@ float p2r_kfact_of(double bz) {
   return (float)(100 / (-0.299792458 * bz));
 }
 
+int p2r_check_aligned(const char* who, unsigned align, std::initializer_list<const void*> ptrs) {
+  int i = 0;
+  for (const void* p : ptrs) {
+    if (p && ((uintptr_t)p % align) != 0)
+      return p2r_set_errorf(P2R_ERR_INVALID, "%s: array argument %d is not %u-byte aligned", who, i, align);
+    ++i;
+  }
+  return P2R_OK;
+}
+
 int p2r_check_config(const p2r_config* cfg, const char* who) {
   if (!cfg) return p2r_set_errorf(P2R_ERR_INVALID, "%s: config is null", who);
   if (cfg->bsize < 1 || cfg->bsize > 4096)

@@ -102,6 +102,7 @@ static int forward_impl(const p2r_config* cfg, const void* trk_in, const void* h
   if (nblocks == 0) return p2r_clear_error();  // an empty batch is valid (pointers unused)
   if (!trk_in || !hits || !trk_out) return p2r_set_errorf(P2R_ERR_INVALID, "%s: null array pointer", who);
   if (trk_in == trk_out) return p2r_set_errorf(P2R_ERR_INVALID, "%s: trk_out may not alias trk_in", who);
+  if ((rc = p2r_check_aligned(who, 4, {trk_in, hits, trk_out, chi2_out, dr, nlay}))) return rc;
   if (cfg->mode != P2R_MODE_RESTART && cfg->mode != P2R_MODE_CHAINED)
     return p2r_set_errorf(P2R_ERR_INVALID, "%s: unknown mode %d", who, cfg->mode);
   if (nlay && cfg->mode != P2R_MODE_CHAINED)
@@ -157,6 +158,7 @@ int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hi
   int rc = p2r_check_config(cfg, "p2r_propagate_to_r");
   if (rc) return rc;
   if (!trk_in || !hits || !trk_out) return p2r_set_error(P2R_ERR_INVALID, "p2r_propagate_to_r: null array pointer");
+  if ((rc = p2r_check_aligned("p2r_propagate_to_r", 4, {trk_in, hits, trk_out, dr}))) return rc;
   if (layer < 0 || layer >= cfg->nlayer)
     return p2r_set_errorf(P2R_ERR_INVALID, "p2r_propagate_to_r: layer %d outside [0, %d)", layer, cfg->nlayer);
   const long long nblocks = (long long)cfg->nevts * cfg->nb;
@@ -176,6 +178,7 @@ int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_
   int rc = p2r_check_config(cfg, "p2r_kalman_update");
   if (rc) return rc;
   if (!trk || !hits) return p2r_set_error(P2R_ERR_INVALID, "p2r_kalman_update: null array pointer");
+  if ((rc = p2r_check_aligned("p2r_kalman_update", 4, {trk, hits, chi2_accum}))) return rc;
   if (layer < 0 || layer >= cfg->nlayer)
     return p2r_set_errorf(P2R_ERR_INVALID, "p2r_kalman_update: layer %d outside [0, %d)", layer, cfg->nlayer);
   const long long nblocks = (long long)cfg->nevts * cfg->nb;
@@ -198,6 +201,8 @@ int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_
 int p2r_count_nonfinite(const void* trk, int64_t nblocks, int32_t bsize, unsigned long long* count_out, void* stream) {
   if (!trk || !count_out) return p2r_set_error(P2R_ERR_INVALID, "p2r_count_nonfinite: null pointer");
   if (nblocks < 0 || bsize < 1) return p2r_set_error(P2R_ERR_INVALID, "p2r_count_nonfinite: bad sizes");
+  if (int rc = p2r_check_aligned("p2r_count_nonfinite", 4, {trk})) return rc;
+  if (int rc = p2r_check_aligned("p2r_count_nonfinite", 8, {count_out})) return rc;
   if (nblocks == 0) return p2r_clear_error();
   const long long ntr = nblocks * (long long)bsize;
   const int threads = 256;

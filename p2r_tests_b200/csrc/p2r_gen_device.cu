@@ -129,6 +129,7 @@ extern "C" int p2r_gen_helix_device(const p2r_gen_params* gp, int32_t bsize, int
   const long long nslots = (long long)nevts * nb * bsize;
   if (nslots == 0) return p2r_clear_error();
   if (!trk_out || !hit_out) return p2r_set_error(P2R_ERR_INVALID, "p2r_gen_helix_device: null array pointer");
+  if (int rc = p2r_check_aligned("p2r_gen_helix_device", 4, {trk_out, hit_out, ntrk_event})) return rc;
   const long long grid = (nslots + 127) / 128;
   if (grid > 0x7fffffffLL) return p2r_set_error(P2R_ERR_INVALID, "p2r_gen_helix_device: too many track slots");
   gen_helix_kernel<<<(unsigned)grid, 128, 0, (cudaStream_t)stream>>>(*gp, bsize, nevts, nb, nlayer, ntrk_event,

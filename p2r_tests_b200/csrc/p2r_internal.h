@@ -2,6 +2,8 @@
 #pragma once
 #include <stdint.h>
 
+#include <initializer_list>
+
 #include "../../include/p2r.h"
 
 // Records `msg` as the calling thread's last error and returns `code`.
@@ -13,6 +15,11 @@ int p2r_clear_error();
 
 // Validates the sizes of a p2r_config; returns P2R_OK or P2R_ERR_INVALID with a message.
 int p2r_check_config(const p2r_config* cfg, const char* who);
+
+// P2R_ERR_INVALID unless every non-null pointer in `ptrs` is a multiple of `align` bytes. The
+// kernels read and write device arrays as 4-byte (8-byte for double and 64-bit counters) words;
+// a misaligned address would fault the kernel, so it is rejected on the host instead.
+int p2r_check_aligned(const char* who, unsigned align, std::initializer_list<const void*> ptrs);
 
 // kfact exactly as the reference rounds it (TBB:654); bz == 0 means 3.8112 T.
 float p2r_kfact_of(double bz);

@@ -60,6 +60,7 @@ extern "C" int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, 
   if (!host_trk_in || !host_hits || !host_trk_out || !dev_trk_in || !dev_hits || !dev_trk_out)
     return p2r_set_error(P2R_ERR_INVALID, "p2r_forward_host: null pointer");
   if (nchunks < 1) return p2r_set_error(P2R_ERR_INVALID, "p2r_forward_host: nchunks must be >= 1");
+  if ((rc = p2r_check_aligned("p2r_forward_host", 4, {dev_trk_in, dev_hits, dev_trk_out}))) return rc;
   if (cfg->nevts == 0 || cfg->nb == 0) return p2r_clear_error();
   StreamPool* pool = nullptr;
   if ((rc = get_pool(&pool))) return rc;

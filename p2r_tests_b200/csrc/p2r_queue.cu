@@ -152,6 +152,9 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
   if (q->nevts == 0 || q->n_items == 0) return p2r_clear_error();
   if (!trk_in || !hits || !trk_out) return p2r_set_errorf(P2R_ERR_INVALID, "%s: null array pointer", who);
   if (((uintptr_t)hits & 15u) != 0) return p2r_set_errorf(P2R_ERR_INVALID, "%s: hits must be 16-byte aligned", who);
+  if ((rc = p2r_check_aligned(who, 4, {trk_in, trk_out, chi2_out, q->nlay_lane})) ||
+      (rc = p2r_check_aligned(who, 8, {event_done_ns, start_ns, q->event_block_offset, q->items})))
+    return rc;
   QueueParams qp;
   qp.f.trk_in = (const float*)trk_in;
   qp.f.hits = (const float*)hits;

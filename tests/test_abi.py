@@ -112,3 +112,28 @@ def test_adjoint_rejects_forward_only_options(p2r):
     assert small < tape5 < tape1
     assert tape1 >= small + 20 * 27 * 8 * 10 * 30 * 32  # 20 FP64 checkpoints per track
     assert l.p2r_forward_backward_workspace_size_tape(ctypes.byref(c), 3) == 0
+
+
+def test_misaligned_device_arrays_rejected(p2r):
+    """Device arrays are read as 4-byte words (8-byte for doubles and 64-bit counters): a
+    misaligned pointer is an INVALID argument on the host, before any launch (runs without a GPU)."""
+    l = p2r.lib()
+    c = _cfg(p2r)
+    odd, ok = 0x10002, 0x10000  # fake device addresses: only their alignment is looked at
+
+    def rejected(rc):
+        return rc == 1 and "aligned" in l.p2r_last_error_string().decode()
+
+    assert rejected(l.p2r_forward(ctypes.byref(c), odd, ok, ok + 64, None, None, None))
+    assert rejected(l.p2r_forward(ctypes.byref(c), ok, ok + 64, ok + 128, odd, None, None))     # chi2_out
+    assert rejected(l.p2r_forward_masked(ctypes.byref(c), ok, ok + 64, ok + 128, odd, None, None, None))
+    assert rejected(l.p2r_propagate_to_r(ctypes.byref(c), ok, odd, 0, ok + 128, None, None))
+    assert rejected(l.p2r_kalman_update(ctypes.byref(c), ok, ok + 64, 0, odd, None))
+    assert rejected(l.p2r_count_nonfinite(odd, 1, 32, ok, None))
+    assert rejected(l.p2r_count_nonfinite(ok, 1, 32, ok + 4, None))                             # 64-bit counter
+    assert rejected(l.p2r_forward_backward(ctypes.byref(c), ok, ok + 64, None, None, ok + 128, None, None, None, None,
+                                           None, ok + 4, None, None, None, 5, 256, 1 << 20, None))  # double grad_dr
+    assert rejected(l.p2r_forward_host(ctypes.byref(c), ok, ok, ok, odd, ok, ok, 4, None))
+    gp = p2r.gen_params()
+    assert rejected(l.p2r_gen_helix_device(ctypes.byref(gp), 32, 1, 1, 20, None, odd, ok, None))
+    assert rejected(l.p2r_fp64_fma_probe(1, 1, 32, ok + 4, None))
