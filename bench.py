@@ -158,6 +158,37 @@ def measured_peaks():
 
 
 # ------------------------------------------------------------------ CPU reference timing
+def accuracy_vs_fp64(trk_ev, hit_ev, ours_ev, nb, bsize, bz, nthreads):
+    """Error of this library's output and of the reference's own CPU output against the FP64
+    oracle on one event of the bench workload (the oracle as the checker). Parameters:
+    |a - f64| / max(|f64|, floor), floor (1, 1, 1, 0.01, 1, 1) for (x, y, z, 1/pT, phi, theta);
+    covariance: |a - f64| / max(|f64|, sqrt(P_ii P_jj)), P the covariance entering the last
+    update. Quantiles over all elements."""
+    from oracle.oracle import Oracle, RefTBB, ref_available
+    f64 = Oracle().run(trk_ev, hit_ev, bsize, NLAYER, 1, bz, "f64")
+    floor = np.array([1.0, 1.0, 1.0, 0.01, 1.0, 1.0])
+    diag = [i * (i + 1) // 2 + i for i in range(6)]
+    d = np.sqrt(np.abs(f64["prior"][:, diag]))
+    scale = np.concatenate([d[:, i:i + 1] * d[:, :i + 1] for i in range(6)], axis=1)  # packed (i, j <= i)
+
+    def errs(out):
+        t = np.ascontiguousarray(out, np.float32).reshape(-1, 28, bsize)
+        par = t[:, 0:6, :].transpose(0, 2, 1).reshape(-1, 6).astype(np.float64)
+        cov = t[:, 6:27, :].transpose(0, 2, 1).reshape(-1, 21).astype(np.float64)
+        ep = np.abs(par - f64["par"]) / np.maximum(np.abs(f64["par"]), floor)
+        ec = np.abs(cov - f64["cov"]) / np.maximum(np.abs(f64["cov"]), scale)
+        q = lambda e: {"p50": float(np.quantile(e, 0.5)), "p99": float(np.quantile(e, 0.99)), "max": float(e.max())}
+        return {"par": q(ep), "cov": q(ec)}
+
+    res = {"sample": f"event 0 of the bench workload ({nb * bsize} tracks x {NLAYER} layers, chained)",
+           "oracle": "own FP64 restatement (oracle/), Bz as the workload", "this_library": errs(ours_ev)}
+    if ref_available(bsize, "kf"):
+        ref = RefTBB(bsize, "kf")
+        ref.set_bz(bz)
+        res["reference_cpu"] = errs(ref.run(trk_ev, hit_ev, 1, nb, NLAYER, True, 1, nthreads))
+    return res
+
+
 def cpu_reference_rate(trk, hit, nevts, nb, bsize, budget_s, nthreads):
     """Times the reference's own driver loop (oracle/_ref) on a bounded sample of events.
     Returns (updates/s, sample description, kind, threads)."""
@@ -624,6 +655,9 @@ def main():
                                                       cfg.bsize, args.cpu_seconds, nthreads)
             cpu = {"value": v, "unit": "track-layer updates/s", "cores": thr, "kind": "reference",
                    "sample": sample + f"; reference build oracle/_ref ({kind}), Bz compiled in at 3.8112 T"}
+            tw, hw = 28 * cfg.bsize * cfg.nb, 9 * cfg.bsize * cfg.nb * NLAYER
+            cpu["accuracy_vs_fp64"] = accuracy_vs_fp64(trk.reshape(-1)[:tw], hit.reshape(-1)[:hw],
+                                                       d_out[:tw].cpu().numpy(), cfg.nb, cfg.bsize, BZ, nthreads)
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "unit": "track-layer updates/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
