@@ -223,7 +223,8 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
 // 32 lanes read and write one 256-byte (double) or 128-byte (float) line per component.
 // Used when the caller's workspace holds the tape (p2r_forward_backward_workspace_size_tape).
 struct TapeParams {
-  void* tape;      // [nslots][27][nthreads] of T: the state before layers 0, CK, 2 CK, ...
+  void* tape;      // [nslots][27][nthreads] of T: the state before layers 0, CK, 2 CK, ...;
+                   // for CK = 1 the state after each layer's propagation, entering its update
   void* segbuf;    // [CK - 1][27][nthreads] of T: the state before layers a+1 .. a+CK-1
   long long nthreads;
 };
@@ -292,10 +293,19 @@ __global__ void __launch_bounds__(kAdjThreads) fwd_tape_kernel(AdjParams p, Tape
   T* tape = (T*)tp.tape;
   T chi2 = 0;
   for (int l = 0; l < c.nl; ++l) {
-    if (l % CK == 0) tape_store(tape + (long long)(l / CK) * 27 * tp.nthreads, tp.nthreads, c.g, par, cov);
     T hp[3], hc[6];
     load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
-    chi2 += adj::layer_fwd(par, cov, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0));
+    if constexpr (CK == 1) {
+      // the propagated state entering the update: the reverse starts each layer from it
+      adj::PropTape<T> t;
+      const T r = adj::hipo(hp[0], hp[1]) + (p.dr ? (T)p.dr[l] : T(0));
+      adj::prop_fwd(par, cov, c.k, c.kinv, r, t, par, cov);
+      tape_store(tape + (long long)l * 27 * tp.nthreads, tp.nthreads, c.g, par, cov);
+      chi2 += adj::upd_fwd(par, cov, hp, hc);
+    } else {
+      if (l % CK == 0) tape_store(tape + (long long)(l / CK) * 27 * tp.nthreads, tp.nthreads, c.g, par, cov);
+      chi2 += adj::layer_fwd(par, cov, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0));
+    }
   }
   if (c.valid) {
     if (p.trk_out) {
@@ -331,7 +341,68 @@ __global__ void __launch_bounds__(kAdjThreads) rev_tape_kernel(AdjParams p, Tape
     if (p.g_chi2) chi2b = (T)p.g_chi2[c.b * bs + c.it];
   }
   T kbar = 0, kinvbar = 0;
-  const int nseg = (c.nl_warp + CK - 1) / CK;
+  if constexpr (CK == 1) {
+    // Layer l, last to first: the update's reverse straight from the tape (the propagated state
+    // entering it), then the state entering the layer (the input track for l = 0, else the
+    // update of layer l-1 applied to its tape entry, as the forward did), the propagation's tape
+    // (its output covariance is not needed, so J C J^T is not recomputed) and its reverse.
+    for (int l = c.nl_warp - 1; l >= 0; --l) {
+      T drb = 0;
+      if (l < c.nl) {
+        T hp[3], hc[6], hpb[3], hcb[6];
+        load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
+        {
+          T up[6], uc[21];
+          tape_load(tape + (long long)l * 27 * tp.nthreads, tp.nthreads, c.g, up, uc);
+          adj::upd_rev(up, uc, hp, hc, pb, cb, chi2b, hpb, hcb);
+        }
+        T sp[6], sc[21];
+        if (l == 0) {
+          const float* tb = p.trk_in + c.b * (long long)(28 * bs);
+#pragma unroll
+          for (int i = 0; i < 6; ++i) sp[i] = (T)tb[i * bs + c.it];
+#pragma unroll
+          for (int i = 0; i < 21; ++i) sc[i] = (T)tb[(6 + i) * bs + c.it];
+        } else {
+          T hq[3], hqc[6];
+          tape_load(tape + (long long)(l - 1) * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
+          load_hit_t(c.hblk + (long long)(l - 1) * (9 * bs), bs, c.it, hq, hqc);
+          adj::upd_fwd(sp, sc, hq, hqc);
+        }
+        const T rh = adj::hipo(hp[0], hp[1]);
+        const T r = rh + (p.dr ? (T)p.dr[l] : T(0));
+        adj::PropTape<T> t;
+        T pp[6], pc[21];
+        adj::prop_fwd(sp, sc, c.k, c.kinv, r, t, pp, pc);
+        T pin[6], cin[21], rbar = 0;
+        adj::prop_rev(t, sp, sc, c.k, c.kinv, r, pb, cb, pin, cin, rbar, kbar, kinvbar);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) pb[i] = pin[i];
+#pragma unroll
+        for (int i = 0; i < 21; ++i) cb[i] = cin[i];
+        drb = rbar;
+        if (rh > T(0)) {
+          const T irh = T(1) / rh;
+          hpb[0] += rbar * hp[0] * irh;
+          hpb[1] += rbar * hp[1] * irh;
+        }
+        if (p.g_hits) {
+          float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
+#pragma unroll
+          for (int i = 0; i < 3; ++i) gh[i * bs + c.it] = (float)hpb[i];
+#pragma unroll
+          for (int i = 0; i < 6; ++i) gh[(3 + i) * bs + c.it] = (float)hcb[i];
+        }
+      } else if (c.valid && p.g_hits) {
+        float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) gh[i * bs + c.it] = 0.f;
+      }
+      drb = warp_sum_t(drb);
+      if (c.lane == 0) wpart[l] = (float)drb;
+    }
+  }
+  const int nseg = CK == 1 ? 0 : (c.nl_warp + CK - 1) / CK;
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int a = seg * CK;
     const int e = min(a + CK, c.nl_warp);
