@@ -1,10 +1,11 @@
 """Forward + adjoint through the C ABI, and a torch.autograd.Function over it.
 
-`forward_backward` calls p2r_forward_backward (one fused launch: chained forward with
-checkpoints, then the hand-written reverse sweep). `P2RChain.apply(trk, hits, dr, bz, cfg,
-ckpt_stride)` returns (trk_out, chi2) from the plain fused forward and, on backward, runs
-the adjoint kernel with the incoming cotangents, giving gradients for the Matriplex track
-and hit arrays (parameter and covariance rows), the per-layer radius offsets dr and Bz.
+`forward_backward` calls p2r_forward_backward (the chained forward with checkpoints, then
+the hand-written reverse sweep). `P2RChain.apply(trk, hits, dr, bz, cfg, ckpt_stride)`
+(ckpt_stride None: auto_ckpt_stride's choice) returns (trk_out, chi2) from the plain fused
+forward and, on backward, runs the adjoint kernel with the incoming cotangents, giving
+gradients for the Matriplex track and hit arrays (parameter and covariance rows), the
+per-layer radius offsets dr and Bz.
 torch is used only for device memory and streams here; the arithmetic is the library's.
 """
 from __future__ import annotations
@@ -31,15 +32,32 @@ def workspace_size(cfg: Config, ckpt_stride: int | None = None) -> int:
     return int(n)
 
 
+def auto_ckpt_stride(cfg: Config, device, tape: bool = True) -> int:
+    """The checkpoint stride used when the caller names none: 1 (the whole state tape, the
+    fastest reverse) when its workspace fits in half the free device memory, else 5; 5 for
+    thread-local checkpoints."""
+    if not tape:
+        return 5
+    free, _ = torch.cuda.mem_get_info(device)
+    return 1 if workspace_size(cfg, 1) <= free // 2 else 5
+
+
 def forward_backward(cfg: Config, trk_in, hits, dr=None, nlay_lane=None, grad_trk_out=None, grad_chi2=None,
-                     ckpt_stride: int = 5, per_event: bool = False, stream=None, out=None, tape: bool = True) -> dict:
+                     ckpt_stride: int | None = None, per_event: bool = False, stream=None, out=None,
+                     tape: bool = True) -> dict:
     """Returns trk_out, chi2, grad_trk_in, grad_hits, grad_dr, grad_bz (and *_event).
     tape: give the library a workspace that holds the checkpoint tape (two-kernel path);
-    False keeps the checkpoints in thread-local memory (smallest workspace). An entry of
-    `out` set to None skips that output (e.g. grad_hits for calibration-only runs)."""
+    False keeps the checkpoints in thread-local memory (smallest workspace). ckpt_stride None:
+    auto_ckpt_stride's choice, made once per `out` dict and kept with its workspace (so repeated
+    calls, a CUDA-graph capture among them, run the same stride). An entry of `out` set to None
+    skips that output (e.g. grad_hits for calibration-only runs)."""
     _check_shapes(cfg, trk_in, hits)
     dev = trk_in.device
     o = out if out is not None else {}
+    if ckpt_stride is None:
+        if o.get("ckpt_stride") is None:
+            o["ckpt_stride"] = auto_ckpt_stride(cfg, dev, tape)
+        ckpt_stride = o["ckpt_stride"]
     f32 = dict(dtype=torch.float32, device=dev)
     f64 = dict(dtype=torch.float64, device=dev)
     o.setdefault("trk_out", torch.empty_like(trk_in))
@@ -73,7 +91,7 @@ class P2RChain(torch.autograd.Function):
     the position and covariance rows of hits, dr and bz."""
 
     @staticmethod
-    def forward(ctx, trk, hits, dr, bz, cfg: Config, ckpt_stride: int = 5):
+    def forward(ctx, trk, hits, dr, bz, cfg: Config, ckpt_stride: int | None = None):
         from .api import forward
         c = Config(**{**cfg.__dict__, "bz": float(bz), "mode": _lib.MODE_CHAINED})
         trk_out = torch.empty_like(trk)
