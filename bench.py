@@ -564,7 +564,7 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         fms_sorted = f0.elapsed_time(f1) / args.calib_steps
-        del o4, t4s, h4s, nl4s
+        del o4
         gc4 = torch.ones(c4.ntracks, dtype=torch.float32, device=dev)
         out4 = {"grad_trk_in": None, "grad_hits": None}
         # checkpoint stride: 1 (the whole state tape, the fastest reverse) when its workspace fits
@@ -590,6 +590,20 @@ def main():
         torch.cuda.synchronize()
         bms = b0.elapsed_time(b1) / args.calib_steps
         ev_sum = out4["grad_dr_event"].sum(0)
+        # the same forward + adjoint on the tracks ordered by layer count (same workspace)
+        out4s = {"grad_trk_in": None, "grad_hits": None, "workspace": out4["workspace"]}
+        p2r.forward_backward(c4, t4s, h4s, dr=dr4, nlay_lane=nl4s, grad_chi2=gc4, per_event=True, out=out4s,
+                             ckpt_stride=ck4, stream=stream)
+        torch.cuda.synchronize()
+        b0.record(stream)
+        for _ in range(args.calib_steps):
+            p2r.forward_backward(c4, t4s, h4s, dr=dr4, nlay_lane=nl4s, grad_chi2=gc4, per_event=True, out=out4s,
+                                 ckpt_stride=ck4, stream=stream)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        bms_sorted = b0.elapsed_time(b1) / args.calib_steps
+        dr_rel = float(((out4s["grad_dr"] - out4["grad_dr"]).abs().max() / out4["grad_dr"].abs().max()).item())
+        del out4s, t4s, h4s, nl4s
         calib = {"workload": f"{c4.ntracks // c4.nevts} tracks x {c4.nevts} events x 40 layers, hits on r = 4..110 cm, "
                              "20-40 layers per track (uniform), dr ~ U[-100, 100] um, generated on the device",
                  "hits_bytes": h4.numel() * 4, "tracks_bytes": t4.numel() * 4, "updates": upd4,
@@ -600,6 +614,11 @@ def main():
                                                        "updates_per_s": upd4 / (fms_sorted / 1e3)}},
                  "forward_adjoint": {"ms_per_step": bms, "ratio_vs_forward": bms / fms, "ckpt_stride": ck4,
                                      "workspace_bytes": p2r.workspace_size(c4, ck4),
+                                     "sorted_by_layer_count": {
+                                         "ms_per_step": bms_sorted,
+                                         "grad_dr_max_rel_diff_vs_unsorted": dr_rel,
+                                         "how": "each event's tracks ordered by layer count (p2r.sort_by_layers_device), "
+                                                "direct calls"},
                                      "api": f"p2r_forward_backward (FP64, ckpt {ck4}), per-event grad_dr/grad_bz, "
                                             "replayed from one CUDA graph"},
                  "per_event_sum_matches_total": bool(torch.allclose(ev_sum, out4["grad_dr"], rtol=1e-10, atol=0)),
