@@ -10,11 +10,12 @@ from .api import (Config, KalmanUpdate, REF_BZ, count_nonfinite, forward, forwar
                   generate_helix, generate_helix_device, kfact, math_check, math_variant, propagateToR, run_layers, summary, tracks_cov, tracks_par, tracks_q)
 
 from .autograd import P2RChain, auto_ckpt_stride, forward_backward, workspace_size
-from .uneven import Queue, inverse, lognormal_counts, permute_tracks, plan, sort_by_layers, sort_by_layers_device, uneven_workload
+from .uneven import (Queue, inverse, inverse_device, lognormal_counts, permute_tracks, permute_tracks_device, plan,
+                     sort_by_layers, sort_by_layers_device, uneven_workload)
 from . import autotune
 
 __all__ = [
-    "P2RChain", "auto_ckpt_stride", "forward_backward", "workspace_size", "Queue", "lognormal_counts", "plan", "uneven_workload", "sort_by_layers", "sort_by_layers_device", "permute_tracks", "inverse",
+    "P2RChain", "auto_ckpt_stride", "forward_backward", "workspace_size", "Queue", "lognormal_counts", "plan", "uneven_workload", "sort_by_layers", "sort_by_layers_device", "permute_tracks", "permute_tracks_device", "inverse", "inverse_device",
     "Config", "KalmanUpdate", "propagateToR", "run_layers", "forward", "forward_host", "fp32_fma_probe", "fp64_fma_probe",
     "count_nonfinite", "kfact", "math_check", "math_variant",
     "gen_params", "generate_helix", "generate_helix_device", "generate_fixture", "summary", "tracks_par", "tracks_cov", "tracks_q",

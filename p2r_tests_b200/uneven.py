@@ -91,6 +91,25 @@ def sort_by_layers_device(cfg: Config, trk, hits, nlay_lane):
     return t, h, nlay_lane[perm].contiguous(), perm
 
 
+def permute_tracks_device(arr, perm, bsize: int, words: int, nlayer: int = 1):
+    """permute_tracks for a flat device tensor (torch): track i of the result is track perm[i]
+    of arr. With perm = inverse_device(p) it undoes the ordering p of sort_by_layers_device,
+    e.g. to return trk_out, grad_trk_in (words 28) or grad_hits (words 9, nlayer) of an ordered
+    run in the caller's track order."""
+    n = perm.numel()
+    nblocks = n // bsize
+    t = arr.view(nblocks, nlayer, words, bsize).permute(0, 3, 1, 2).reshape(n, nlayer, words)[perm]
+    return t.reshape(nblocks, bsize, nlayer, words).permute(0, 2, 3, 1).contiguous().view(-1)
+
+
+def inverse_device(perm):
+    """Inverse of a device permutation (torch): inv[perm[i]] = i."""
+    import torch
+    inv = torch.empty_like(perm)
+    inv[perm] = torch.arange(perm.numel(), device=perm.device, dtype=perm.dtype)
+    return inv
+
+
 def inverse(perm: np.ndarray) -> np.ndarray:
     inv = np.empty_like(perm)
     inv[perm] = np.arange(len(perm))

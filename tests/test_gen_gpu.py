@@ -67,3 +67,7 @@ def test_device_sort_by_layers_matches_host():
     p2r.forward(cfg, ts, hs, b, nlay_lane=ns)
     back = p2r.permute_tracks(b.cpu().numpy(), p2r.inverse(ph), 32, 28)
     assert np.array_equal(bits(back), bits(a.cpu().numpy()))
+    # the same round trip on the device, for tracks and hits
+    inv = p2r.inverse_device(perm)
+    assert np.array_equal(bits(p2r.permute_tracks_device(b, inv, 32, 28).cpu().numpy()), bits(a.cpu().numpy()))
+    assert torch.equal(p2r.permute_tracks_device(hs, inv, 32, 9, cfg.nlayer), hit)
