@@ -429,6 +429,26 @@ def main():
             barrier()
             ams = max_over_ranks(a0.elapsed_time(a1)) / args.adj_steps
             fp32[str(ck)] = {"ms_per_step": ams, "ratio_vs_forward": ams / ms_per_step}
+        # thread-local checkpoints (the smallest workspace; the path of the allocation-free
+        # entry point)
+        tl, wstl = {}, {}
+        for ck in (5, 10):
+            for _ in range(2):
+                p2r.forward_backward(cfg, d_trk, d_hit, dr=d_dr, grad_trk_out=g_trk, grad_chi2=g_chi2,
+                                     ckpt_stride=ck, stream=stream, out=wstl, tape=False)
+            torch.cuda.synchronize()
+            barrier()
+            a0.record(stream)
+            for _ in range(args.adj_steps):
+                p2r.forward_backward(cfg, d_trk, d_hit, dr=d_dr, grad_trk_out=g_trk, grad_chi2=g_chi2,
+                                     ckpt_stride=ck, stream=stream, out=wstl, tape=False)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            ams = max_over_ranks(a0.elapsed_time(a1)) / args.adj_steps
+            tl[str(ck)] = {"ms_per_step": ams, "ratio_vs_forward": ams / ms_per_step}
+        adjoint["thread_local_checkpoints"] = {"ckpt_stride": tl, "workspace_bytes": p2r.workspace_size(cfg)}
+        del wstl
         adjoint["fp32_instance"] = {"ckpt_stride": fp32,
                                     "note": "P2R_FLAG_ADJ_FP32, same tape kernels in float; per-track gradients "
                                             "~1e-3 at the median, shared Bz gradient ~17 % off: below the 1e-3 bar"}
