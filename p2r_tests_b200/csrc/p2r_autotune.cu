@@ -14,10 +14,13 @@ extern "C" int p2r_autotune_forward(const p2r_config* cfg, const void* trk_in, c
   if (!cfg || !threads || !stages || !out || n_threads < 1 || n_stages < 1 || reps < 1)
     return p2r_set_error(P2R_ERR_INVALID, "p2r_autotune_forward: bad arguments");
   cudaStream_t st = (cudaStream_t)stream;
-  cudaEvent_t e0, e1;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
-  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_autotune_forward: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return p2r_set_errorf(P2R_ERR_CUDA, "p2r_autotune_forward: %s", cudaGetErrorString(e));
+  }
   out->best_ms = FLT_MAX;
   out->block_threads = 0;
   out->stages = 0;
@@ -30,15 +33,18 @@ extern "C" int p2r_autotune_forward(const p2r_config* cfg, const void* trk_in, c
       c.stages = stages[j];
       rc = p2r_forward(&c, trk_in, hits, trk_out, nullptr, nullptr, stream);
       if (rc) break;
-      cudaEventRecord(e0, st);
-      for (int r = 0; r < reps && rc == P2R_OK; ++r) rc = p2r_forward(&c, trk_in, hits, trk_out, nullptr, nullptr, stream);
-      cudaEventRecord(e1, st);
-      if ((e = cudaEventSynchronize(e1)) != cudaSuccess) {
+      if ((e = cudaEventRecord(e0, st)) != cudaSuccess) {
         rc = p2r_set_errorf(P2R_ERR_CUDA, "p2r_autotune_forward: %s", cudaGetErrorString(e));
         break;
       }
+      for (int r = 0; r < reps && rc == P2R_OK; ++r) rc = p2r_forward(&c, trk_in, hits, trk_out, nullptr, nullptr, stream);
+      if (rc) break;
       float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
+      if ((e = cudaEventRecord(e1, st)) != cudaSuccess || (e = cudaEventSynchronize(e1)) != cudaSuccess ||
+          (e = cudaEventElapsedTime(&ms, e0, e1)) != cudaSuccess) {
+        rc = p2r_set_errorf(P2R_ERR_CUDA, "p2r_autotune_forward: %s", cudaGetErrorString(e));
+        break;
+      }
       ms /= reps;
       if (out->n_tried < 64) {
         out->tried_threads[out->n_tried] = threads[i];
