@@ -611,6 +611,7 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
                          double* grad_dr_event, double* grad_bz_event, int32_t ckpt_stride, void* workspace,
                          size_t workspace_bytes, void* stream) {
   const char* who = "p2r_forward_backward";
+  P2rRange range(who);
   int rc = p2r_check_config(cfg, who);
   if (rc) return rc;
   if (cfg->mode != P2R_MODE_CHAINED) return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: only CHAINED mode has an adjoint", who);

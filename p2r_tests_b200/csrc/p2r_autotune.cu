@@ -13,6 +13,7 @@ extern "C" int p2r_autotune_forward(const p2r_config* cfg, const void* trk_in, c
                                     int32_t n_stages, int32_t reps, p2r_tune_result* out, void* stream) {
   if (!cfg || !threads || !stages || !out || n_threads < 1 || n_stages < 1 || reps < 1)
     return p2r_set_error(P2R_ERR_INVALID, "p2r_autotune_forward: bad arguments");
+  P2rRange range("p2r_autotune_forward");
   cudaStream_t st = (cudaStream_t)stream;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);

@@ -96,6 +96,7 @@ static int check_ptr16(const void* ptr) { return ((uintptr_t)ptr & 15u) == 0; }
 
 static int forward_impl(const p2r_config* cfg, const void* trk_in, const void* hits, void* trk_out,
                         const int32_t* nlay, float* chi2_out, const float* dr, void* stream, const char* who) {
+  P2rRange range(who);
   int rc = p2r_check_config(cfg, who);
   if (rc) return rc;
   const long long nblocks = (long long)cfg->nevts * cfg->nb;
@@ -155,6 +156,7 @@ int p2r_forward_masked(const p2r_config* cfg, const void* trk_in, const void* hi
 
 int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hits, int32_t layer, void* trk_out,
                        const float* dr, void* stream) {
+  P2rRange range("p2r_propagate_to_r");
   int rc = p2r_check_config(cfg, "p2r_propagate_to_r");
   if (rc) return rc;
   if (!trk_in || !hits || !trk_out) return p2r_set_error(P2R_ERR_INVALID, "p2r_propagate_to_r: null array pointer");
@@ -175,6 +177,7 @@ int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hi
 
 int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_t layer, float* chi2_accum,
                       void* stream) {
+  P2rRange range("p2r_kalman_update");
   int rc = p2r_check_config(cfg, "p2r_kalman_update");
   if (rc) return rc;
   if (!trk || !hits) return p2r_set_error(P2R_ERR_INVALID, "p2r_kalman_update: null array pointer");

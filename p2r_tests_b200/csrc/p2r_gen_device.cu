@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(128) gen_helix_kernel(p2r_gen_params gp, int b
 extern "C" int p2r_gen_helix_device(const p2r_gen_params* gp, int32_t bsize, int64_t nevts, int64_t nb,
                                     int32_t nlayer, const int32_t* ntrk_event, void* trk_out, void* hit_out,
                                     void* stream) {
+  P2rRange range("p2r_gen_helix_device");
   if (!gp) return p2r_set_error(P2R_ERR_INVALID, "p2r_gen_helix_device: null parameters");
   if (bsize < 1 || nevts < 0 || nb < 0 || nlayer < 1 || gp->bz == 0.0 || gp->r_last <= gp->r_first)
     return p2r_set_error(P2R_ERR_INVALID, "p2r_gen_helix_device: bad sizes or geometry");

@@ -4,6 +4,8 @@
 
 #include <initializer_list>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/p2r.h"
 
 // Records `msg` as the calling thread's last error and returns `code`.
@@ -20,6 +22,15 @@ int p2r_check_config(const p2r_config* cfg, const char* who);
 // kernels read and write device arrays as 4-byte (8-byte for double and 64-bit counters) words;
 // a misaligned address would fault the kernel, so it is rejected on the host instead.
 int p2r_check_aligned(const char* who, unsigned align, std::initializer_list<const void*> ptrs);
+
+// Names an entry point's span on a profiler's host timeline (an NVTX range: header-only, a
+// no-op unless a tool such as Nsight Systems or Nsight Compute is attached).
+struct P2rRange {
+  explicit P2rRange(const char* name) { nvtxRangePushA(name); }
+  ~P2rRange() { nvtxRangePop(); }
+  P2rRange(const P2rRange&) = delete;
+  P2rRange& operator=(const P2rRange&) = delete;
+};
 
 // kfact exactly as the reference rounds it (TBB:654); bz == 0 means 3.8112 T.
 float p2r_kfact_of(double bz);

@@ -55,6 +55,7 @@ int get_pool(StreamPool** out) {
 extern "C" int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void* host_hits,
                                 void* host_trk_out, void* dev_trk_in, void* dev_hits, void* dev_trk_out,
                                 int32_t nchunks, void* stream) {
+  P2rRange range("p2r_forward_host");
   int rc = p2r_check_config(cfg, "p2r_forward_host");
   if (rc) return rc;
   if (!host_trk_in || !host_hits || !host_trk_out || !dev_trk_in || !dev_hits || !dev_trk_out)

@@ -143,6 +143,7 @@ int check_queue(const p2r_queue* q, const char* who) {
 int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
                   unsigned long long* event_done_ns, unsigned long long* start_ns, void* workspace, size_t ws_bytes,
                   cudaStream_t st, const char* who) {
+  P2rRange range(who);
   int rc = check_queue(q, who);
   if (rc) return rc;
   const QueueWs w = queue_ws(q->nevts);
