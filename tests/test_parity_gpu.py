@@ -467,22 +467,25 @@ def test_host_buffer_pipeline_from_two_threads(p2r, torch):
 
 
 EDGE_REGIMES = {"low_pt": dict(pt=1.0), "high_pt": dict(pt=50.0),
-                "forward": dict(theta_min=0.1, theta_max=0.3), "backward": dict(theta_min=2.84, theta_max=3.04)}
+                "forward": dict(theta_min=0.1, theta_max=0.3), "backward": dict(theta_min=2.84, theta_max=3.04),
+                "bz_2T": dict(bz=2.0), "bz_4.5T": dict(bz=4.5)}
 
 
 @pytest.mark.parametrize("regime", list(EDGE_REGIMES))
 @pytest.mark.parametrize("mode", list(MODES))
 def test_edge_regimes_accuracy_vs_live_reference(p2r, oracle, torch, regime, mode):
-    """Tracks outside the default workload's ranges: pT 1 and 50 GeV, and polar angles near the
-    beam axis (0.1-0.3 and 2.84-3.04 rad). Against the FP64 oracle the GPU is at least as accurate
+    """Tracks outside the default workload's ranges: pT 1 and 50 GeV, polar angles near the
+    beam axis (0.1-0.3 and 2.84-3.04 rad), and fields of 2 and 4.5 T. Against the FP64 oracle the GPU is at least as accurate
     as the reference's own CPU build at every error quantile (within ACC_FACTOR), over the tracks
     that all three keep finite, and keeps at least as many tracks finite up to 0.5 % of them (near
     the axis about 1 % of chained tracks go non-finite in the reference and in FP64 as well)."""
     ref = ref_or_none(32, "kf")
     if ref is None:
         pytest.skip("reference build not present")
-    cfg = p2r.Config(bsize=32, nlayer=20, nevts=2, nb=30, bz=3.8, mode=MODES[mode])
-    trk, hit = p2r.generate_helix(cfg, p2r.gen_params(bz=3.8, seed=77, **EDGE_REGIMES[regime]))
+    kw = dict(EDGE_REGIMES[regime])
+    bz = kw.pop("bz", 3.8)
+    cfg = p2r.Config(bsize=32, nlayer=20, nevts=2, nb=30, bz=bz, mode=MODES[mode])
+    trk, hit = p2r.generate_helix(cfg, p2r.gen_params(bz=bz, seed=77, **kw))
     ref.set_bz(cfg.bz)
     rout = ref.run(trk, hit, cfg.nevts, cfg.nb, cfg.nlayer, chained=bool(MODES[mode]))
     out = gpu_forward(p2r, torch, cfg, trk, hit)
