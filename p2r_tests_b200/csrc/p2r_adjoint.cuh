@@ -456,39 +456,39 @@ P2R_UNROLL
   pb_in[5] = thetab;
 }
 
-// KalmanUpdate of (p, c) with hit (hp, hc), forward in the reference's operation order
-// (TBB:433-642); returns chi2. The determinant is taken in double (TBB:457).
+// KalmanUpdate of (p, c) with hit (hp, hc): the reference's formulas (TBB:433-642) with the two
+// quotients by 2 rh taken as one reciprocal and the rows of H*C (u = R00 C_m0 + R01 C_m1, v = C_m2)
+// formed once for the gain and for C - K*(H*C), as the FP32 forward does; returns chi2. The
+// determinant is taken in double (TBB:457).
 template <class T>
 P2R_HD T upd_fwd(T (&p)[6], T (&c)[21], const T (&hp)[3], const T (&hc)[6]) {
   const T rh = hipo(hp[0], hp[1]);
-  const T R00 = -(hp[1] + p[1]) / (T(2) * rh);
-  const T R01 = (hp[0] + p[0]) / (T(2) * rh);
+  const T ih = T(0.5f) / rh;
+  const T R00 = -(hp[1] + p[1]) * ih;
+  const T R01 = (hp[0] + p[0]) * ih;
   const T e0 = (R00 * (c[0] + hc[0]) + R01 * (c[1] + hc[1])) * R00 + (R00 * (c[1] + hc[1]) + R01 * (c[2] + hc[2])) * R01;
   const T e1 = (c[3] + hc[3]) * R00 + (c[4] + hc[4]) * R01;
   const T e2 = c[5] + hc[5];
   const double det = (double)e0 * e2 - (double)e1 * e1;
   const T s = T(1.0 / det);
   const T i0 = s * e2, i1 = e1 * -s, i2 = s * e0;
-  T K0[6], K1[6];
+  T u[6], v[6], K0[6], K1[6];
 P2R_UNROLL
   for (int m = 0; m < 6; ++m) {
-    const T cm0 = c[S6(m, 0)], cm1 = c[S6(m, 1)], cm2 = c[S6(m, 2)];
-    K0[m] = cm0 * (R00 * i0) + cm1 * (R01 * i0) + cm2 * i1;
-    K1[m] = cm0 * (R00 * i1) + cm1 * (R01 * i1) + cm2 * i2;
+    u[m] = R00 * c[S6(m, 0)] + R01 * c[S6(m, 1)];
+    v[m] = c[S6(m, 2)];
+    K0[m] = u[m] * i0 + v[m] * i1;
+    K1[m] = u[m] * i1 + v[m] * i2;
   }
   const T res0 = R00 * (hp[0] - p[0]) + R01 * (hp[1] - p[1]);
   const T res1 = hp[2] - p[2];
   const T chi2 = i0 * res0 * res0 + T(2) * i1 * res0 * res1 + i2 * res1 * res1;
 P2R_UNROLL
   for (int m = 0; m < 6; ++m) p[m] = p[m] + K0[m] * res0 + K1[m] * res1;
-  T nc[21];
 P2R_UNROLL
   for (int i = 0; i < 6; ++i)
 P2R_UNROLL
-    for (int j = 0; j <= i; ++j)
-      nc[S6(i, j)] = c[S6(i, j)] - (K0[i] * R00 * c[S6(0, j)] + K0[i] * R01 * c[S6(1, j)] + K1[i] * c[S6(2, j)]);
-P2R_UNROLL
-  for (int i = 0; i < 21; ++i) c[i] = nc[i];
+    for (int j = 0; j <= i; ++j) c[S6(i, j)] = c[S6(i, j)] - (K0[i] * u[j] + K1[i] * v[j]);
   return chi2;
 }
 
