@@ -142,22 +142,27 @@ P2R_UNROLL
   sincos4(t.alpha, t.sa, t.ca, t.omc);
   const T cP = t.cP, sP = t.sP, ca = t.ca, sa = t.sa, alpha = t.alpha;
   const T dadx = t.dadx, dady = t.dady, dadipt = t.dadipt, dadphi = t.dadphi;
-  t.J00 = T(1) + k * dadx * (cP * ca - sP * sa) * pt;
-  t.J01 = k * dady * (cP * ca - sP * sa) * pt;
-  t.J03 = k * (cP * (iptin * dadipt * ca - sa) + sP * (t.omc - iptin * dadipt * sa)) * pt * pt;
-  t.J04 = k * (cP * dadphi * ca - sP * dadphi * sa - sP * sa + cP * ca - cP) * pt;
-  t.J10 = k * dadx * (sP * ca + cP * sa) * pt;
-  t.J11 = T(1) + k * dady * (sP * ca + cP * sa) * pt;
-  t.J13 = k * (sP * (iptin * dadipt * ca - sa) + cP * (iptin * dadipt * sa - t.omc)) * pt * pt;
-  t.J14 = k * (sP * dadphi * ca + cP * dadphi * sa + sP * ca + cP * sa - sP) * pt;
+  // TBB:753-807 with their shared factors formed once: U = cos(phi + alpha), V = sin(phi + alpha),
+  // w = ipt dadipt, k pt; e.g. J03 = k (cP (w ca - sa) + sP (omc - w sa)) pt^2 = k pt^2 (w U - V + sP)
+  const T U = cP * ca - sP * sa, V = sP * ca + cP * sa, w = iptin * dadipt, d1 = dadphi + T(1);
+  const T kp = k * pt, kp2 = kp * pt;
+  t.J00 = T(1) + dadx * U * kp;
+  t.J01 = dady * U * kp;
+  t.J03 = (w * U - V + sP) * kp2;
+  t.J04 = (d1 * U - cP) * kp;
+  t.J10 = dadx * V * kp;
+  t.J11 = T(1) + dady * V * kp;
+  t.J13 = (w * V + U - cP) * kp2;
+  t.J14 = (d1 * V - sP) * kp;
   sincos_(thetain, &t.sT, &t.cT);
   t.isT = T(1) / t.sT;
   const T cT = t.cT, isT = t.isT;
-  t.J20 = k * cT * dadx * pt * isT;
-  t.J21 = k * cT * dady * pt * isT;
-  t.J23 = k * cT * (iptin * dadipt - alpha) * pt * pt * isT;
-  t.J24 = k * dadphi * cT * pt * isT;
-  t.J25 = -k * alpha * pt * isT * isT;
+  const T G = kp * cT * isT;  // rows 2 and 4 share (dadx, dady, ., ., dadphi, .): J2 = G (those) + ...
+  t.J20 = G * dadx;
+  t.J21 = G * dady;
+  t.J23 = G * pt * (w - alpha);
+  t.J24 = G * dadphi;
+  t.J25 = -kp * alpha * isT * isT;
   t.J40 = dadx;
   t.J41 = dady;
   t.J43 = dadipt;
@@ -171,8 +176,9 @@ P2R_UNROLL
             c5 = ic[S6(5, j)];
     T0[j] = t.J00 * c0 + t.J01 * c1 + t.J03 * c3 + t.J04 * c4;
     T1[j] = t.J10 * c0 + t.J11 * c1 + t.J13 * c3 + t.J14 * c4;
-    T2[j] = t.J20 * c0 + t.J21 * c1 + c2 + t.J23 * c3 + t.J24 * c4 + t.J25 * c5;
-    T4[j] = t.J40 * c0 + t.J41 * c1 + t.J43 * c3 + t.J44 * c4;
+    const T n = dadx * c0 + dady * c1 + dadphi * c4;  // row 4 = n + dadipt c3 + c4, row 2 = G n + ...
+    T2[j] = G * n + c2 + t.J23 * c3 + t.J25 * c5;
+    T4[j] = n + dadipt * c3 + c4;
   }
   // C' = (J C) J^T, lower triangle
 P2R_UNROLL
@@ -183,10 +189,12 @@ P2R_UNROLL
       Ti[j] = i == 0 ? T0[j] : i == 1 ? T1[j] : i == 2 ? T2[j] : i == 4 ? T4[j] : ic[S6(i, j)];
     oc[S6(i, 0)] = Ti[0] * t.J00 + Ti[1] * t.J01 + Ti[3] * t.J03 + Ti[4] * t.J04;
     if (i >= 1) oc[S6(i, 1)] = Ti[0] * t.J10 + Ti[1] * t.J11 + Ti[3] * t.J13 + Ti[4] * t.J14;
-    if (i >= 2)
-      oc[S6(i, 2)] = Ti[0] * t.J20 + Ti[1] * t.J21 + Ti[2] + Ti[3] * t.J23 + Ti[4] * t.J24 + Ti[5] * t.J25;
+    if (i >= 2) {
+      const T n = Ti[0] * dadx + Ti[1] * dady + Ti[4] * dadphi;
+      oc[S6(i, 2)] = G * n + Ti[2] + Ti[3] * t.J23 + Ti[5] * t.J25;
+      if (i >= 4) oc[S6(i, 4)] = n + Ti[3] * dadipt + Ti[4];
+    }
     if (i >= 3) oc[S6(i, 3)] = Ti[3];
-    if (i >= 4) oc[S6(i, 4)] = Ti[0] * t.J40 + Ti[1] * t.J41 + Ti[3] * t.J43 + Ti[4] * t.J44;
     if (i >= 5) oc[S6(i, 5)] = Ti[5];
   }
   op[0] = xo;
