@@ -219,9 +219,12 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
 // recomputed segment states in a tape in device memory instead of thread-local arrays:
 // fwd_tape_kernel runs the forward and stores the state every CK layers; rev_tape_kernel
 // walks the segments backwards, recomputes each segment's states once into a segment
-// buffer, and reverses the layers. Layout of both: [slot][27 components][thread], so a warp's
-// 32 lanes read and write one 256-byte (double) or 128-byte (float) line per component.
-// Used when the caller's workspace holds the tape (p2r_forward_backward_workspace_size_tape).
+// buffer, and reverses the layers. At CK = 1 every layer has a slot, and the slot holds the
+// propagated state entering the layer's update instead: the reverse starts each layer from it
+// and rebuilds the layer's input with one update of the previous slot. Layout of both:
+// [slot][27 components][thread], so a warp's 32 lanes read and write one 256-byte (double) or
+// 128-byte (float) line per component. Used when the caller's workspace holds the tape
+// (p2r_forward_backward_workspace_size_tape).
 struct TapeParams {
   void* tape;      // [nslots][27][nthreads] of T: the state before layers 0, CK, 2 CK, ...;
                    // for CK = 1 the state after each layer's propagation, entering its update
