@@ -37,13 +37,21 @@ int get_pool(StreamPool** out) {
   std::lock_guard<std::mutex> lk(g_pool_mu);
   StreamPool& p = g_pools[dev];
   if (!p.ready) {
-    for (int i = 0; i < kPoolStreams; ++i) {
-      if ((e = cudaStreamCreateWithFlags(&p.s[i], cudaStreamNonBlocking)) != cudaSuccess ||
-          (e = cudaEventCreateWithFlags(&p.join[i], cudaEventDisableTiming)) != cudaSuccess)
-        return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_host: %s", cudaGetErrorString(e));
+    for (int i = 0; i < kPoolStreams; ++i) p.s[i] = nullptr, p.join[i] = nullptr;
+    p.fork = nullptr;
+    for (int i = 0; i < kPoolStreams && e == cudaSuccess; ++i) {
+      e = cudaStreamCreateWithFlags(&p.s[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.join[i], cudaEventDisableTiming);
     }
-    if ((e = cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming)) != cudaSuccess)
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming);
+    if (e != cudaSuccess) {  // release what was created, so a later call starts from nothing
+      for (int i = 0; i < kPoolStreams; ++i) {
+        if (p.join[i]) cudaEventDestroy(p.join[i]);
+        if (p.s[i]) cudaStreamDestroy(p.s[i]);
+      }
+      if (p.fork) cudaEventDestroy(p.fork);
       return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_host: %s", cudaGetErrorString(e));
+    }
     p.ready = true;
   }
   *out = &p;
