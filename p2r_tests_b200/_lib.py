@@ -11,6 +11,7 @@ from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libp2r_b200.so"
+ABI_VERSION = 1  # P2R_ABI_VERSION of include/p2r.h, which these signatures follow
 
 P2R_OK = 0
 P2R_ERR_INVALID = 1
@@ -151,6 +152,9 @@ def lib() -> ctypes.CDLL:
             fn = getattr(l, name)
             fn.restype = res
             fn.argtypes = args
+        if l.p2r_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} reports ABI version {l.p2r_abi_version()}, these bindings follow "
+                               f"{ABI_VERSION}: rebuild with `python -m p2r_tests_b200.build`")
         _lib = l
     return _lib
 

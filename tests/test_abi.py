@@ -31,6 +31,8 @@ def test_binding_covers_header(p2r):
 
 def test_abi_version_and_kfact(p2r):
     assert p2r.lib().p2r_abi_version() == 1
+    header = (ROOT / "include" / "p2r.h").read_text()
+    assert f"#define P2R_ABI_VERSION {p2r._lib.ABI_VERSION}" in header
     # kfact as the reference rounds its constant (TBB:654): float(100/(-0.299792458*3.8112))
     assert np.float32(p2r.kfact(3.8112)) == np.float32(100 / (-0.299792458 * 3.8112))
     assert p2r.kfact(0.0) == p2r.kfact(3.8112)
