@@ -119,7 +119,12 @@ int main(int argc, char** argv) {
   bool help = false;
   if (!parse(argc, argv, a, help)) return 1;
   if (help) return usage(argv[0]);
-  if (a.bsize < 1 || a.ntrks < a.bsize || a.nevts < 1 || a.nlayer < 1 || a.niter < 1) {
+  if (p2r_abi_version() != P2R_ABI_VERSION) {  // a library from another header loaded at run time
+    std::fprintf(stderr, "libp2r_b200 ABI version %d, this program was built for %d\n", p2r_abi_version(),
+                 P2R_ABI_VERSION);
+    return 1;
+  }
+  if (a.bsize < 1|| a.ntrks < a.bsize || a.nevts < 1 || a.nlayer < 1 || a.niter < 1) {
     std::fprintf(stderr, "bad sizes\n");
     return 1;
   }
