@@ -21,7 +21,10 @@ def shard_events(nevts: int, world: int, rank: int) -> tuple[int, int]:
 def shard_uneven(ntrk_event, world: int, rank: int) -> tuple[int, int]:
     """Contiguous event range balancing the TRACK count (prefix split of the cumulative
     counts at multiples of total/world), for batches with uneven events."""
-    c = np.concatenate([[0], np.cumsum(np.asarray(ntrk_event, np.int64))])
+    counts = np.asarray(ntrk_event, np.int64).reshape(-1)
+    if world < 1 or not 0 <= rank < world or (counts < 0).any():
+        raise ValueError("bad world/rank or negative track count")
+    c = np.concatenate([[0], np.cumsum(counts)])
     total = c[-1]
     cut = lambda r: int(np.searchsorted(c, total * r / world, side="left")) if r < world else len(c) - 1
     return cut(rank), cut(rank + 1)
@@ -30,6 +33,8 @@ def shard_uneven(ntrk_event, world: int, rank: int) -> tuple[int, int]:
 def event_slice(arr: np.ndarray, e0: int, e1: int, nevts: int) -> np.ndarray:
     """The rows of a Matriplex array (tracks or hits, event-major) that belong to [e0, e1)."""
     flat = np.ascontiguousarray(arr).reshape(-1)
+    if nevts < 1 or flat.size % nevts or not 0 <= e0 <= e1 <= nevts:
+        raise ValueError(f"event range [{e0}, {e1}) of {nevts} events over {flat.size} words")
     per = flat.size // nevts
     return flat[e0 * per:e1 * per]
 

@@ -27,6 +27,26 @@ def test_shard_events_partitions():
     assert ranges[0][0] == 0 and ranges[-1][1] == len(counts) and ranges[0][1] == ranges[1][0]
     load = [counts[s:e].sum() for s, e in ranges]
     assert max(load) <= counts.sum() * 0.5 + counts.max()
+    rng = np.random.default_rng(4)
+    for world in (1, 3, 8):
+        c = rng.integers(0, 500, 37)
+        ranges = [shard_uneven(c, world, r) for r in range(world)]
+        assert ranges[0][0] == 0 and ranges[-1][1] == len(c)
+        assert all(a[1] == b[0] and a[0] <= a[1] for a, b in zip(ranges, ranges[1:]))
+        assert max(c[s:e].sum() for s, e in ranges) <= c.sum() / world + c.max()
+    for bad in ((counts, 0, 0), (counts, 2, 2), (counts, 2, -1), ([3, -1], 1, 0)):
+        with pytest.raises(ValueError):
+            shard_uneven(*bad)
+
+
+def test_event_slice_is_the_events_byte_range():
+    from p2r_tests_b200.distributed import event_slice
+    a = np.arange(5 * 12, dtype=np.float32).reshape(5, 12)
+    assert np.array_equal(event_slice(a, 1, 3, 5), a[1:3].reshape(-1))
+    assert event_slice(a, 2, 2, 5).size == 0
+    for bad in ((0, 1, 0), (0, 6, 5), (3, 2, 5), (0, 1, 7)):
+        with pytest.raises(ValueError):
+            event_slice(a, *bad)
 
 
 def _grad_on_tracks(par0, cov0, q, hpos, hcov, dr, bz):
