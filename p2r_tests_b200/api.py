@@ -74,6 +74,21 @@ def _ptr(t) -> int | None:
     return int(t)
 
 
+def _arg(t, dtype: str, numel: int | None, name: str) -> int | None:
+    """Device pointer of an optional array argument, after checking that it is a `dtype`
+    tensor of at least `numel` elements: the library reads or writes that many elements of
+    that type behind the pointer and cannot see the tensor's own size or type."""
+    if t is None:
+        return None
+    if hasattr(t, "dtype"):
+        import torch
+        if t.dtype != getattr(torch, dtype):
+            raise P2RError(_lib.P2R_ERR_INVALID, f"{name}: {t.dtype} tensor given, torch.{dtype} expected")
+        if numel is not None and t.numel() < numel:
+            raise P2RError(_lib.P2R_ERR_INVALID, f"{name}: {t.numel()} elements given, {numel} needed")
+    return _ptr(t)
+
+
 def _stream(stream) -> int | None:
     if stream is None:
         import torch
@@ -82,6 +97,9 @@ def _stream(stream) -> int | None:
 
 
 def _check_shapes(cfg: Config, trk, hits) -> None:
+    for t in (trk, hits):
+        if t is not None and hasattr(t, "dtype") and str(t.dtype) != "torch.float32":
+            raise P2RError(_lib.P2R_ERR_INVALID, f"Matriplex arrays are float32 tensors, {t.dtype} given")
     if trk is not None and hasattr(trk, "numel") and trk.numel() != cfg.nblocks * TRK_WORDS * cfg.bsize:
         raise P2RError(_lib.P2R_ERR_INVALID,
                        f"track array has {trk.numel()} words, expected {cfg.nblocks * TRK_WORDS * cfg.bsize}")
@@ -95,16 +113,16 @@ def propagateToR(cfg: Config, trk_in, hits, layer: int, trk_out, dr=None, stream
     _check_shapes(cfg, trk_in, hits)
     _check_shapes(cfg, trk_out, None)
     c = cfg.c()
-    check(lib().p2r_propagate_to_r(ctypes.byref(c), _ptr(trk_in), _ptr(hits), layer, _ptr(trk_out), _ptr(dr),
-                                   _stream(stream)))
+    check(lib().p2r_propagate_to_r(ctypes.byref(c), _ptr(trk_in), _ptr(hits), layer, _ptr(trk_out),
+                                   _arg(dr, "float32", cfg.nlayer, "dr"), _stream(stream)))
 
 
 def KalmanUpdate(cfg: Config, trk, hits, layer: int, chi2_accum=None, stream=None) -> None:
     """KalmanUpdate (TBB:433-642) of every block with its hit in `layer`, in place (TBB:911)."""
     _check_shapes(cfg, trk, hits)
     c = cfg.c()
-    check(lib().p2r_kalman_update(ctypes.byref(c), _ptr(trk), _ptr(hits), layer, _ptr(chi2_accum),
-                                  _stream(stream)))
+    check(lib().p2r_kalman_update(ctypes.byref(c), _ptr(trk), _ptr(hits), layer,
+                                  _arg(chi2_accum, "float32", cfg.ntracks, "chi2_accum"), _stream(stream)))
 
 
 def run_layers(cfg: Config, trk_in, hits, trk_out, stream=None) -> None:
@@ -122,12 +140,14 @@ def forward(cfg: Config, trk_in, hits, trk_out, chi2=None, dr=None, nlay_lane=No
     _check_shapes(cfg, trk_in, hits)
     _check_shapes(cfg, trk_out, None)
     c = cfg.c()
+    p_chi2, p_dr = _arg(chi2, "float32", cfg.ntracks, "chi2"), _arg(dr, "float32", cfg.nlayer, "dr")
     if nlay_lane is None:
-        check(lib().p2r_forward(ctypes.byref(c), _ptr(trk_in), _ptr(hits), _ptr(trk_out), _ptr(chi2), _ptr(dr),
+        check(lib().p2r_forward(ctypes.byref(c), _ptr(trk_in), _ptr(hits), _ptr(trk_out), p_chi2, p_dr,
                                 _stream(stream)))
     else:
-        check(lib().p2r_forward_masked(ctypes.byref(c), _ptr(trk_in), _ptr(hits), _ptr(trk_out), _ptr(nlay_lane),
-                                       _ptr(chi2), _ptr(dr), _stream(stream)))
+        check(lib().p2r_forward_masked(ctypes.byref(c), _ptr(trk_in), _ptr(hits), _ptr(trk_out),
+                                       _arg(nlay_lane, "int32", cfg.ntracks, "nlay_lane"), p_chi2, p_dr,
+                                       _stream(stream)))
 
 
 def forward_host(cfg: Config, host_trk_in: np.ndarray, host_hits: np.ndarray, host_trk_out: np.ndarray,
@@ -150,13 +170,14 @@ def forward_host(cfg: Config, host_trk_in: np.ndarray, host_hits: np.ndarray, ho
 def fp32_fma_probe(out, iters: int, blocks: int, threads: int = 256, stream=None, packed: bool = False) -> int:
     """Launches the FP32 FMA probe (packed: the f32x2 form); returns the FLOPs it performs."""
     fn = lib().p2r_fp32x2_fma_probe if packed else lib().p2r_fp32_fma_probe
-    check(fn(iters, blocks, threads, _ptr(out), _stream(stream)))
+    check(fn(iters, blocks, threads, _arg(out, "float32", blocks * threads, "out"), _stream(stream)))
     return 64 * iters * blocks * threads
 
 
 def fp64_fma_probe(out, iters: int, blocks: int, threads: int = 256, stream=None) -> int:
     """Launches the FP64 FMA probe (out: float64, blocks*threads); returns the FLOPs it performs."""
-    check(lib().p2r_fp64_fma_probe(iters, blocks, threads, _ptr(out), _stream(stream)))
+    check(lib().p2r_fp64_fma_probe(iters, blocks, threads, _arg(out, "float64", blocks * threads, "out"),
+                                   _stream(stream)))
     return 64 * iters * blocks * threads
 
 
@@ -169,14 +190,16 @@ def math_check(a, b, stream=None):
     """The hot path's own a / b and sqrt(a) on the device (float32 tensors of one size)."""
     import torch
     quot, root = torch.empty_like(a), torch.empty_like(a)
-    check(lib().p2r_math_check(a.numel(), _ptr(a), _ptr(b), _ptr(quot), _ptr(root), _stream(stream)))
+    check(lib().p2r_math_check(a.numel(), _arg(a, "float32", None, "a"), _arg(b, "float32", a.numel(), "b"),
+                               _ptr(quot), _ptr(root), _stream(stream)))
     return quot, root
 
 
 def count_nonfinite(trk, nblocks: int, bsize: int, stream=None) -> int:
     import torch
     cnt = torch.zeros(1, dtype=torch.int64, device=trk.device)
-    check(lib().p2r_count_nonfinite(_ptr(trk), nblocks, bsize, _ptr(cnt), _stream(stream)))
+    check(lib().p2r_count_nonfinite(_arg(trk, "float32", nblocks * TRK_WORDS * bsize, "trk"), nblocks, bsize,
+                                    _ptr(cnt), _stream(stream)))
     return int(cnt.item())
 
 

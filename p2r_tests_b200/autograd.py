@@ -16,7 +16,7 @@ import torch
 
 from . import _lib
 from ._lib import P2RError, check, lib
-from .api import Config, HIT_WORDS, TRK_WORDS, _check_shapes, _ptr, _stream
+from .api import Config, HIT_WORDS, TRK_WORDS, _arg, _check_shapes, _ptr, _stream
 
 
 def workspace_size(cfg: Config, ckpt_stride: int | None = None) -> int:
@@ -75,11 +75,17 @@ def forward_backward(cfg: Config, trk_in, hits, dr=None, nlay_lane=None, grad_tr
         ws = torch.empty(need, dtype=torch.uint8, device=dev)
         o["workspace"] = ws
     c = cfg.c()
+    ntrk, nt, nh, nl = cfg.ntracks, trk_in.numel(), hits.numel(), cfg.nlayer
     check(lib().p2r_forward_backward(
-        ctypes.byref(c), _ptr(trk_in), _ptr(hits), _ptr(dr), _ptr(nlay_lane), _ptr(o["trk_out"]), _ptr(o["chi2"]),
-        _ptr(grad_trk_out), _ptr(grad_chi2), _ptr(o["grad_trk_in"]), _ptr(o["grad_hits"]), _ptr(o["grad_dr"]),
-        _ptr(o["grad_bz"]), _ptr(o.get("grad_dr_event")), _ptr(o.get("grad_bz_event")), ckpt_stride, _ptr(ws),
-        ws.numel(), _stream(stream)))
+        ctypes.byref(c), _ptr(trk_in), _ptr(hits), _arg(dr, "float32", nl, "dr"),
+        _arg(nlay_lane, "int32", ntrk, "nlay_lane"), _arg(o["trk_out"], "float32", nt, "trk_out"),
+        _arg(o["chi2"], "float32", ntrk, "chi2"), _arg(grad_trk_out, "float32", nt, "grad_trk_out"),
+        _arg(grad_chi2, "float32", ntrk, "grad_chi2"), _arg(o["grad_trk_in"], "float32", nt, "grad_trk_in"),
+        _arg(o["grad_hits"], "float32", nh, "grad_hits"), _arg(o["grad_dr"], "float64", nl, "grad_dr"),
+        _arg(o["grad_bz"], "float64", 1, "grad_bz"),
+        _arg(o.get("grad_dr_event"), "float64", cfg.nevts * nl, "grad_dr_event"),
+        _arg(o.get("grad_bz_event"), "float64", cfg.nevts, "grad_bz_event"), ckpt_stride,
+        _arg(ws, "uint8", need, "workspace"), ws.numel(), _stream(stream)))
     return o
 
 

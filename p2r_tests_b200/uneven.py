@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import CQueue, CQueueItem, P2RError, check, lib
-from .api import Config, _ptr, _stream, gen_params, generate_helix
+from .api import Config, HIT_WORDS, TRK_WORDS, _arg, _ptr, _stream, gen_params, generate_helix
 
 
 def lognormal_counts(nevts: int, median: float = 2000.0, sigma: float = 1.0, lo: int = 50, hi: int = 20000,
@@ -155,8 +155,16 @@ class Queue:
         self.start_ns = torch.zeros(1, dtype=torch.int64, device=self.dev)
         self.graph = None
 
+    def _arrays(self, trk_in, hits, trk_out, chi2):
+        """The four array pointers, each checked for type and size against the workload."""
+        w = self.w
+        ntrk = w["nblocks"] * w["bsize"]
+        return (_arg(trk_in, "float32", ntrk * TRK_WORDS, "trk_in"),
+                _arg(hits, "float32", ntrk * w["nlayer"] * HIT_WORDS, "hits"),
+                _arg(trk_out, "float32", ntrk * TRK_WORDS, "trk_out"), _arg(chi2, "float32", ntrk, "chi2"))
+
     def run(self, trk_in, hits, trk_out, chi2=None, stream=None) -> None:
-        check(lib().p2r_run_queue(ctypes.byref(self.q), _ptr(trk_in), _ptr(hits), _ptr(trk_out), _ptr(chi2),
+        check(lib().p2r_run_queue(ctypes.byref(self.q), *self._arrays(trk_in, hits, trk_out, chi2),
                                   _ptr(self.done_ns), _ptr(self.start_ns), _ptr(self.ws), self.ws.numel(),
                                   _stream(stream)))
 
@@ -164,7 +172,7 @@ class Queue:
         """Captures the launch sequence into a CUDA graph (pointers are baked in)."""
         self.release()
         g = ctypes.c_void_p()
-        check(lib().p2r_queue_graph_create(ctypes.byref(self.q), _ptr(trk_in), _ptr(hits), _ptr(trk_out), _ptr(chi2),
+        check(lib().p2r_queue_graph_create(ctypes.byref(self.q), *self._arrays(trk_in, hits, trk_out, chi2),
                                            _ptr(self.done_ns), _ptr(self.start_ns), _ptr(self.ws), self.ws.numel(),
                                            ctypes.byref(g)))
         self.graph = g

@@ -139,3 +139,46 @@ def test_misaligned_device_arrays_rejected(p2r):
     gp = p2r.gen_params()
     assert rejected(l.p2r_gen_helix_device(ctypes.byref(gp), 32, 1, 1, 20, None, odd, ok, None))
     assert rejected(l.p2r_fp64_fma_probe(1, 1, 32, ok + 4, None))
+
+
+def test_bindings_check_array_types_and_sizes(p2r, monkeypatch):
+    """The library sees bare pointers, so the Python bindings check each tensor's type and
+    size first: a float16 track array or a short radius-offset vector would otherwise be read
+    or written past its end. Pointer and stream extraction are replaced by None here (no GPU), so a call
+    whose tensors pass the checks reaches the library and stops at its null-pointer check."""
+    import torch
+    from p2r_tests_b200 import api, autograd
+    for mod in (api, autograd):
+        monkeypatch.setattr(mod, "_ptr", lambda t: None)
+        monkeypatch.setattr(mod, "_stream", lambda s: None)
+    cfg = p2r.Config(bsize=32, nlayer=4, nevts=1, nb=2)
+    f32 = lambda n, dt=torch.float32: torch.zeros(n, dtype=dt)
+    trk, hit = f32(cfg.nblocks * 28 * 32), f32(cfg.nblocks * 4 * 9 * 32)
+    out, chi2, dr, nlay = torch.zeros_like(trk), f32(cfg.ntracks), f32(4), torch.zeros(cfg.ntracks, dtype=torch.int32)
+
+    def fails(fn, *words):
+        with pytest.raises(p2r.P2RError) as e:
+            fn()
+        msg = str(e.value)
+        assert all(w in msg for w in words), msg
+
+    fails(lambda: p2r.forward(cfg, trk, hit, out, chi2=chi2, dr=dr, nlay_lane=nlay), "null")  # checks pass
+    fails(lambda: p2r.forward(cfg, trk.half().repeat(2)[:trk.numel()], hit, out), "float32", "float16")
+    fails(lambda: p2r.forward(cfg, trk, hit, out.double()), "float64")
+    fails(lambda: p2r.forward(cfg, trk, hit, out, dr=dr.double()), "dr", "float64")
+    fails(lambda: p2r.forward(cfg, trk, hit, out, dr=dr[:3]), "dr", "3 elements", "4 needed")
+    fails(lambda: p2r.forward(cfg, trk, hit, out, chi2=chi2[:-1]), "chi2")
+    fails(lambda: p2r.forward(cfg, trk, hit, out, nlay_lane=nlay.long()), "nlay_lane", "int64")
+    fails(lambda: p2r.propagateToR(cfg, trk, hit, 0, out, dr=dr.half()), "dr")
+    fails(lambda: p2r.KalmanUpdate(cfg, out, hit, 0, chi2_accum=chi2.double()), "chi2_accum")
+    fails(lambda: p2r.count_nonfinite(trk[:-1], cfg.nblocks, 32), "trk", "needed")
+    fails(lambda: p2r.fp64_fma_probe(f32(256), 1, 1, 256), "out", "float32")
+
+    def adj(**out_entries):
+        o = {"grad_hits": None, **out_entries}
+        return p2r.forward_backward(cfg, trk, hit, dr=dr, grad_chi2=chi2, ckpt_stride=5, out=o)
+    fails(lambda: adj(), "null input")  # checks pass
+    fails(lambda: adj(grad_dr=f32(4)), "grad_dr", "float32")
+    fails(lambda: adj(grad_trk_in=f32(trk.numel() - 1)), "grad_trk_in", "needed")
+    fails(lambda: p2r.forward_backward(cfg, trk, hit, dr=dr, grad_chi2=chi2, ckpt_stride=5, per_event=True,
+                                       out={"grad_bz_event": f32(0, torch.float64)}), "grad_bz_event")
