@@ -154,8 +154,8 @@ def forward_host(cfg: Config, host_trk_in: np.ndarray, host_hits: np.ndarray, ho
                  dev_trk_in, dev_hits, dev_trk_out, nchunks: int = 8, stream=None) -> None:
     """Fused forward from HOST arrays to a HOST array, copies overlapped with kernels in chunks."""
     for a in (host_trk_in, host_hits, host_trk_out):
-        if not (isinstance(a, np.ndarray) and a.flags.c_contiguous):
-            raise P2RError(_lib.P2R_ERR_INVALID, "host arrays must be C-contiguous numpy arrays")
+        if not (isinstance(a, np.ndarray) and a.flags.c_contiguous and a.dtype == np.float32):
+            raise P2RError(_lib.P2R_ERR_INVALID, "host arrays must be C-contiguous float32 numpy arrays")
     _check_shapes(cfg, dev_trk_in, dev_hits)
     _check_shapes(cfg, dev_trk_out, None)
     if host_trk_in.nbytes != cfg.nblocks * TRK_WORDS * cfg.bsize * 4 or host_trk_out.nbytes != host_trk_in.nbytes \

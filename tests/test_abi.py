@@ -174,6 +174,10 @@ def test_bindings_check_array_types_and_sizes(p2r, monkeypatch):
     fails(lambda: p2r.count_nonfinite(trk[:-1], cfg.nblocks, 32), "trk", "needed")
     fails(lambda: p2r.fp64_fma_probe(f32(256), 1, 1, 256), "out", "float32")
 
+    h_trk, h_hit = trk.numpy(), hit.numpy()
+    fails(lambda: p2r.forward_host(cfg, h_trk, h_hit, h_trk.copy(), trk, hit, out), "null")  # checks pass
+    fails(lambda: p2r.forward_host(cfg, h_trk.view(np.float64), h_hit, h_trk.copy(), trk, hit, out), "float32")
+
     def adj(**out_entries):
         o = {"grad_hits": None, **out_entries}
         return p2r.forward_backward(cfg, trk, hit, dr=dr, grad_chi2=chi2, ckpt_stride=5, out=o)
