@@ -37,7 +37,7 @@ def _store(key: str, value: dict) -> None:
     p = cache_path()
     try:
         p.parent.mkdir(parents=True, exist_ok=True)
-        tmp = p.with_suffix(".tmp")
+        tmp = p.with_suffix(f".{os.getpid()}.tmp")  # one per process: ranks may store at once
         tmp.write_text(json.dumps(c, indent=1, sort_keys=True))
         os.replace(tmp, p)
     except OSError:
@@ -63,7 +63,10 @@ def tune_forward(cfg: Config, trk: np.ndarray, hit: np.ndarray, bsizes=(32, 64, 
     must be divisible by every bsize tried)."""
     import torch
     ntr_ev = cfg.nb * cfg.bsize
-    key = f"{_gpu_name()}|forward|ntr_ev={ntr_ev}|nevts={cfg.nevts}|nlayer={cfg.nlayer}|mode={cfg.mode}"
+    if not any(ntr_ev % bs == 0 for bs in bsizes):
+        raise ValueError(f"no bsize of {tuple(bsizes)} divides the {ntr_ev} tracks per event")
+    key = (f"{_gpu_name()}|forward|ntr_ev={ntr_ev}|nevts={cfg.nevts}|nlayer={cfg.nlayer}|mode={cfg.mode}"
+           f"|flags={cfg.flags}|space={tuple(bsizes)}x{tuple(threads)}x{tuple(stages)}")
     if use_cache and key in _load_cache():
         return _load_cache()[key]
     th = np.array(threads, np.int32)
@@ -101,7 +104,7 @@ def tune_queue(ntrk_event, bsizes=(32, 64, 128), granularity=(1, 2, 4, 8, 16), t
     from .uneven import Queue, uneven_workload
     counts = np.asarray(ntrk_event, np.int64)
     sig = f"nevts={len(counts)}|ntr={int(counts.sum())}|median={int(np.median(counts))}|nlay={nlayer_max}"
-    key = f"{_gpu_name()}|queue|{sig}"
+    key = f"{_gpu_name()}|queue|{sig}|space={tuple(bsizes)}x{tuple(granularity)}x{tuple(threads)}x{tuple(stages)}"
     if use_cache and key in _load_cache():
         return _load_cache()[key]
     results = []

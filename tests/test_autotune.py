@@ -38,8 +38,16 @@ def test_cache_store_load_and_corrupt_file(p2r, tmp_path, monkeypatch):
     autotune._store("gpu|forward|x", {"bsize": 64, "ms": 0.5})
     autotune._store("gpu|queue|y", {"bsize": 32, "ms": 1.5})
     assert autotune._load_cache() == {"gpu|forward|x": {"bsize": 64, "ms": 0.5}, "gpu|queue|y": {"bsize": 32, "ms": 1.5}}
+    assert sorted(x.name for x in f.parent.iterdir()) == ["tune.json"]  # no temporary file left
     f.write_text("{not json")
     assert autotune._load_cache() == {}
+
+
+def test_tune_forward_rejects_widths_that_split_events(p2r):
+    from p2r_tests_b200 import autotune
+    cfg = p2r.Config(bsize=32, nlayer=4, nevts=2, nb=3)  # 96 tracks per event
+    with pytest.raises(ValueError, match="divides"):
+        autotune.tune_forward(cfg, None, None, bsizes=(64, 128))
 
 
 def test_native_tuner_rejects_bad_arguments(p2r):
