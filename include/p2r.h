@@ -146,7 +146,11 @@ int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void*
  * MPHIT blocks lay + b*nlayer as usual (nlayer = layer slots per block, the largest layer
  * count). Lane `it` of block b runs nlay_lane[b*bsize + it] layers (0 for padding lanes),
  * CHAINED. Work items (host-planned by p2r_queue_plan, copied to the device) are claimed
- * by a persistent grid with one atomic counter; no thread waits on another. */
+ * by a persistent grid with one atomic counter; no thread waits on another.
+ * The items and event offsets are device data and are not re-read on the host: each item
+ * must cover blocks [block0, block0 + nblk) inside [0, nblocks) and inside its event's range,
+ * which p2r_queue_plan guarantees for non-decreasing offsets from 0 to nblocks. Layer counts
+ * are clamped to [0, nlayer] on the device. */
 typedef struct p2r_queue_item {
   int32_t event; /* event of the range */
   int32_t nblk;  /* blocks in the range */
