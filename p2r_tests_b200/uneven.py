@@ -140,12 +140,21 @@ class Queue:
         self.torch = torch
         self.w = w
         self.dev = torch.device(device)
-        items = plan(w["event_block_offset"], blocks_per_item)
+        # the kernel reads int64 offsets and int32 layer counts and trusts the block ranges
+        off = np.ascontiguousarray(w["event_block_offset"], np.int64)
+        nlay = np.ascontiguousarray(w["nlay_lane"], np.int32).reshape(-1)
+        if off.ndim != 1 or len(off) < 1 or off[0] != 0 or off[-1] != w["nblocks"] or (np.diff(off) < 0).any():
+            raise ValueError("event_block_offset must rise from 0 to nblocks")
+        if nlay.size != w["nblocks"] * w["bsize"]:
+            raise ValueError(f"nlay_lane has {nlay.size} entries, nblocks * bsize = {w['nblocks'] * w['bsize']}")
+        items = plan(off, blocks_per_item)
         self.n_items = len(items)
-        self.d_off = torch.from_numpy(w["event_block_offset"]).to(self.dev)
+        self.d_off = torch.from_numpy(off).to(self.dev)
         self.d_items = torch.from_numpy(items.view(np.uint8).copy()).to(self.dev)
-        self.d_nlay = torch.from_numpy(w["nlay_lane"]).to(self.dev)
-        self.nevts = len(w["ntrk_event"])
+        self.d_nlay = torch.from_numpy(nlay).to(self.dev)
+        self.nevts = len(off) - 1
+        if "ntrk_event" in w and len(w["ntrk_event"]) != self.nevts:
+            raise ValueError("ntrk_event and event_block_offset disagree on the event count")
         self.q = CQueue(w["bsize"], w["nlayer"], self.nevts, w["nblocks"], w["bz"], flags, block_threads, stages,
                         ctas_per_sm, self.d_off.data_ptr(), self.d_items.data_ptr(), self.n_items,
                         self.d_nlay.data_ptr())

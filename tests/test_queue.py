@@ -30,6 +30,14 @@ def test_queue_rejects_bad_description(p2r):
     assert l.p2r_run_queue(ctypes.byref(q), None, None, None, None, None, None, None, 0, None) == p2r._lib.P2R_ERR_QUEUE
     q = p2r._lib.CQueue(32, 25, 1, 4, 3.8, 0, 0, 0, 0, None, None, 1, None)  # blocks but no arrays
     assert l.p2r_run_queue(ctypes.byref(q), None, None, None, None, None, None, None, 0, None) == p2r._lib.P2R_ERR_QUEUE
+    # the Python description is checked before anything reaches the device
+    w = p2r.uneven_workload(np.array([33, 64, 1, 50]), bsize=32)
+    bad = [dict(w, event_block_offset=np.array([1, 2, 4, 5, 7])), dict(w, event_block_offset=np.array([0, 2, 4, 5, 6])),
+           dict(w, event_block_offset=np.array([0, 4, 2, 5, 7])), dict(w, nlay_lane=w["nlay_lane"][:-1]),
+           dict(w, ntrk_event=w["ntrk_event"][:-1])]
+    for b in bad:
+        with pytest.raises(ValueError):
+            p2r.Queue(b, device="cpu")
 
 
 def test_uneven_workload_padding(p2r):
