@@ -45,6 +45,15 @@ int p2r_check_aligned(const char* who, unsigned align, std::initializer_list<con
   return P2R_OK;
 }
 
+int p2r_check_disjoint(const char* who, const char* what, const void* a, size_t na, const void* b, size_t nb,
+                       bool allow_same) {
+  if (!a || !b || na == 0 || nb == 0) return P2R_OK;
+  if (allow_same && a == b && na == nb) return P2R_OK;
+  const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+  if (x < y + nb && y < x + na) return p2r_set_errorf(P2R_ERR_INVALID, "%s: %s overlap", who, what);
+  return P2R_OK;
+}
+
 int p2r_check_config(const p2r_config* cfg, const char* who) {
   if (!cfg) return p2r_set_errorf(P2R_ERR_INVALID, "%s: config is null", who);
   if (cfg->bsize < 1 || cfg->bsize > 4096)

@@ -108,6 +108,21 @@ static int forward_impl(const p2r_config* cfg, const void* trk_in, const void* h
     return p2r_set_errorf(P2R_ERR_INVALID, "%s: unknown mode %d", who, cfg->mode);
   if (nlay && cfg->mode != P2R_MODE_CHAINED)
     return p2r_set_errorf(P2R_ERR_INVALID, "%s: per-lane layer counts need CHAINED mode", who);
+  {
+    const size_t tb = (size_t)nblocks * 28 * cfg->bsize * sizeof(float);
+    const size_t hb = (size_t)nblocks * cfg->nlayer * 9 * cfg->bsize * sizeof(float);
+    const size_t lb = (size_t)nblocks * cfg->bsize * sizeof(float);  // chi2 and layer counts
+    if ((rc = p2r_check_disjoint(who, "trk_out and trk_in", trk_out, tb, trk_in, tb)) ||
+        (rc = p2r_check_disjoint(who, "trk_out and hits", trk_out, tb, hits, hb)) ||
+        (rc = p2r_check_disjoint(who, "trk_out and nlay_lane", trk_out, tb, nlay, lb)) ||
+        (rc = p2r_check_disjoint(who, "trk_out and dr", trk_out, tb, dr, cfg->nlayer * sizeof(float))) ||
+        (rc = p2r_check_disjoint(who, "chi2_out and trk_out", chi2_out, lb, trk_out, tb)) ||
+        (rc = p2r_check_disjoint(who, "chi2_out and trk_in", chi2_out, lb, trk_in, tb)) ||
+        (rc = p2r_check_disjoint(who, "chi2_out and hits", chi2_out, lb, hits, hb)) ||
+        (rc = p2r_check_disjoint(who, "chi2_out and nlay_lane", chi2_out, lb, nlay, lb)) ||
+        (rc = p2r_check_disjoint(who, "chi2_out and dr", chi2_out, lb, dr, cfg->nlayer * sizeof(float))))
+      return rc;
+  }
   FwdParams p;
   p.trk_in = (const float*)trk_in;
   p.hits = (const float*)hits;
@@ -165,6 +180,12 @@ int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hi
     return p2r_set_errorf(P2R_ERR_INVALID, "p2r_propagate_to_r: layer %d outside [0, %d)", layer, cfg->nlayer);
   const long long nblocks = (long long)cfg->nevts * cfg->nb;
   if (nblocks == 0) return p2r_clear_error();
+  const size_t tb = (size_t)nblocks * 28 * cfg->bsize * sizeof(float);
+  const size_t hb = (size_t)nblocks * cfg->nlayer * 9 * cfg->bsize * sizeof(float);
+  if ((rc = p2r_check_disjoint("p2r_propagate_to_r", "trk_out and trk_in", trk_out, tb, trk_in, tb, true)) ||
+      (rc = p2r_check_disjoint("p2r_propagate_to_r", "trk_out and hits", trk_out, tb, hits, hb)) ||
+      (rc = p2r_check_disjoint("p2r_propagate_to_r", "trk_out and dr", trk_out, tb, dr, cfg->nlayer * sizeof(float))))
+    return rc;
   const long long ntr = nblocks * cfg->bsize;
   const int threads = 128;
   propagate_kernel<<<(unsigned)((ntr + threads - 1) / threads), threads, 0, (cudaStream_t)stream>>>(
@@ -186,6 +207,13 @@ int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_
     return p2r_set_errorf(P2R_ERR_INVALID, "p2r_kalman_update: layer %d outside [0, %d)", layer, cfg->nlayer);
   const long long nblocks = (long long)cfg->nevts * cfg->nb;
   if (nblocks == 0) return p2r_clear_error();
+  const size_t tb = (size_t)nblocks * 28 * cfg->bsize * sizeof(float);
+  const size_t hb = (size_t)nblocks * cfg->nlayer * 9 * cfg->bsize * sizeof(float);
+  const size_t lb = (size_t)nblocks * cfg->bsize * sizeof(float);
+  if ((rc = p2r_check_disjoint("p2r_kalman_update", "trk and hits", trk, tb, hits, hb)) ||
+      (rc = p2r_check_disjoint("p2r_kalman_update", "chi2_accum and trk", chi2_accum, lb, trk, tb)) ||
+      (rc = p2r_check_disjoint("p2r_kalman_update", "chi2_accum and hits", chi2_accum, lb, hits, hb)))
+    return rc;
   const long long ntr = nblocks * cfg->bsize;
   const int threads = 128;
   const unsigned grid = (unsigned)((ntr + threads - 1) / threads);

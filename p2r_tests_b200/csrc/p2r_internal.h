@@ -1,5 +1,6 @@
 // Internal helpers shared by the library's translation units (not part of the ABI).
 #pragma once
+#include <stddef.h>
 #include <stdint.h>
 
 #include <initializer_list>
@@ -22,6 +23,14 @@ int p2r_check_config(const p2r_config* cfg, const char* who);
 // kernels read and write device arrays as 4-byte (8-byte for double and 64-bit counters) words;
 // a misaligned address would fault the kernel, so it is rejected on the host instead.
 int p2r_check_aligned(const char* who, unsigned align, std::initializer_list<const void*> ptrs);
+
+// P2R_ERR_INVALID when the byte ranges [a, a + na) and [b, b + nb) share a byte, naming them
+// by `what`. A written array that overlaps another array of the same launch would let one
+// track's writes land in another track's inputs. With allow_same, a = b with na = nb is
+// accepted: in-place use, where every thread reads and writes only its own track's words.
+// Null pointers and empty ranges overlap nothing.
+int p2r_check_disjoint(const char* who, const char* what, const void* a, size_t na, const void* b, size_t nb,
+                       bool allow_same = false);
 
 // Names an entry point's span on a profiler's host timeline (an NVTX range: header-only, a
 // no-op unless a tool such as Nsight Systems or Nsight Compute is attached).

@@ -71,6 +71,14 @@ extern "C" int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, 
   if (nchunks < 1) return p2r_set_error(P2R_ERR_INVALID, "p2r_forward_host: nchunks must be >= 1");
   if ((rc = p2r_check_aligned("p2r_forward_host", 4, {dev_trk_in, dev_hits, dev_trk_out}))) return rc;
   if (cfg->nevts == 0 || cfg->nb == 0) return p2r_clear_error();
+  {  // the copies write dev_trk_in and dev_hits, the kernels dev_trk_out: all three disjoint
+    const size_t tb = (size_t)cfg->nevts * cfg->nb * 28 * cfg->bsize * sizeof(float);
+    const size_t hb = (size_t)cfg->nevts * cfg->nb * cfg->nlayer * 9 * cfg->bsize * sizeof(float);
+    if ((rc = p2r_check_disjoint("p2r_forward_host", "dev_trk_in and dev_trk_out", dev_trk_in, tb, dev_trk_out, tb)) ||
+        (rc = p2r_check_disjoint("p2r_forward_host", "dev_hits and dev_trk_out", dev_hits, hb, dev_trk_out, tb)) ||
+        (rc = p2r_check_disjoint("p2r_forward_host", "dev_trk_in and dev_hits", dev_trk_in, tb, dev_hits, hb)))
+      return rc;
+  }
   StreamPool* pool = nullptr;
   if ((rc = get_pool(&pool))) return rc;
   std::lock_guard<std::mutex> lk(pool->mu);

@@ -31,6 +31,16 @@ def pytest_collection_modifyitems(config, items):
             item.add_marker(skip)
 
 
+@pytest.fixture
+def host_only():
+    """For tests that hand the library fake device addresses to see its host-side checks
+    reject them: they run only where no GPU is visible. A call that a check let through would
+    reach a kernel launch, which fails harmlessly without a device but would touch those
+    addresses on a GPU."""
+    if _cuda_available():
+        pytest.skip("fake device addresses are passed only on hosts without a GPU")
+
+
 @pytest.fixture(scope="session")
 def p2r():
     import p2r_tests_b200 as m

@@ -45,6 +45,7 @@ def _cfg(p2r, **kw):
     return c.c()
 
 
+@pytest.mark.usefixtures("host_only")
 @pytest.mark.parametrize("bad,code", [
     (dict(bsize=0), 1), (dict(bsize=5000), 1), (dict(nlayer=0), 1), (dict(nevts=-1), 1), (dict(mode=7), 1),
     (dict(block_threads=100), 1), (dict(stages=9), 1),
@@ -57,6 +58,7 @@ def test_forward_rejects_bad_config(p2r, bad, code):
     assert l.p2r_last_error_string().decode()
 
 
+@pytest.mark.usefixtures("host_only")
 def test_forward_rejects_null_and_alias(p2r):
     l = p2r.lib()
     c = _cfg(p2r)
@@ -66,6 +68,7 @@ def test_forward_rejects_null_and_alias(p2r):
     assert l.p2r_forward(None, 16, 32, 48, None, None, None) == 1
 
 
+@pytest.mark.usefixtures("host_only")
 def test_per_layer_rejects_bad_layer(p2r):
     l = p2r.lib()
     c = _cfg(p2r)
@@ -74,6 +77,7 @@ def test_per_layer_rejects_bad_layer(p2r):
     assert "layer" in l.p2r_last_error_string().decode()
 
 
+@pytest.mark.usefixtures("host_only")
 def test_masked_needs_chained_and_counts(p2r):
     l = p2r.lib()
     c = _cfg(p2r, mode=0)
@@ -82,6 +86,7 @@ def test_masked_needs_chained_and_counts(p2r):
     assert l.p2r_forward_masked(ctypes.byref(c), 16, 32, 48, None, None, None, None) == 1
 
 
+@pytest.mark.usefixtures("host_only")
 def test_empty_work_is_ok_without_gpu(p2r):
     """nevts*nb == 0 returns OK before touching the device (an empty batch is valid)."""
     l = p2r.lib()
@@ -89,6 +94,7 @@ def test_empty_work_is_ok_without_gpu(p2r):
     assert l.p2r_forward(ctypes.byref(c), 16, 32, 48, None, None, None) == 0
 
 
+@pytest.mark.usefixtures("host_only")
 def test_generators_reject_bad_args(p2r):
     l = p2r.lib()
     gp = p2r.gen_params()
@@ -99,6 +105,7 @@ def test_generators_reject_bad_args(p2r):
                              buf.ctypes.data, buf.ctypes.data) == 1  # nlayer > input hits
 
 
+@pytest.mark.usefixtures("host_only")
 def test_adjoint_rejects_forward_only_options(p2r):
     """squash-phi is a forward-only option; the adjoint refuses it before any device work,
     and the tape workspace size grows with the tape and is reported for valid strides only."""
@@ -116,6 +123,7 @@ def test_adjoint_rejects_forward_only_options(p2r):
     assert l.p2r_forward_backward_workspace_size_tape(ctypes.byref(c), 3) == 0
 
 
+@pytest.mark.usefixtures("host_only")
 def test_misaligned_device_arrays_rejected(p2r):
     """Device arrays are read as 4-byte words (8-byte for doubles and 64-bit counters): a
     misaligned pointer is an INVALID argument on the host, before any launch (runs without a GPU)."""
@@ -141,6 +149,7 @@ def test_misaligned_device_arrays_rejected(p2r):
     assert rejected(l.p2r_fp64_fma_probe(1, 1, 32, ok + 4, None))
 
 
+@pytest.mark.usefixtures("host_only")
 def test_bindings_check_array_types_and_sizes(p2r, monkeypatch):
     """The library sees bare pointers, so the Python bindings check each tensor's type and
     size first: a float16 track array or a short radius-offset vector would otherwise be read
@@ -186,3 +195,41 @@ def test_bindings_check_array_types_and_sizes(p2r, monkeypatch):
     fails(lambda: adj(grad_trk_in=f32(trk.numel() - 1)), "grad_trk_in", "needed")
     fails(lambda: p2r.forward_backward(cfg, trk, hit, dr=dr, grad_chi2=chi2, ckpt_stride=5, per_event=True,
                                        out={"grad_bz_event": f32(0, torch.float64)}), "grad_bz_event")
+
+
+@pytest.mark.usefixtures("host_only")
+def test_overlapping_arrays_rejected(p2r):
+    """A written array may not share bytes with another array of the same call (one track's
+    writes would land in another's inputs); the per-layer propagation may run exactly in place.
+    Only the fake addresses' byte ranges are compared, on the host (runs without a GPU)."""
+    l = p2r.lib()
+    c = _cfg(p2r)  # one block of 32 tracks, 20 layers
+    tb, hb, lb = 28 * 32 * 4, 20 * 9 * 32 * 4, 32 * 4
+    base = 1 << 32
+    t_in, hits, t_out = base, base + (1 << 20), base + (2 << 20)
+
+    def overlap(rc, *words):
+        msg = l.p2r_last_error_string().decode()
+        return rc == 1 and "overlap" in msg and all(w in msg for w in words)
+
+    assert overlap(l.p2r_forward(ctypes.byref(c), t_in, hits, t_in + 256, None, None, None), "trk_in")
+    assert overlap(l.p2r_forward(ctypes.byref(c), t_in, hits, hits + hb - 256, None, None, None), "hits")
+    assert overlap(l.p2r_forward(ctypes.byref(c), t_in, hits, t_out, t_out + tb - 64, None, None), "chi2_out")
+    assert overlap(l.p2r_forward(ctypes.byref(c), t_in, hits, t_out, t_in, None, None), "chi2_out", "trk_in")
+    assert overlap(l.p2r_forward_masked(ctypes.byref(c), t_in, hits, t_out, t_out + 64, None, None, None), "nlay")
+    assert overlap(l.p2r_propagate_to_r(ctypes.byref(c), t_in, hits, 0, t_in + 128, None, None), "trk_in")
+    assert overlap(l.p2r_propagate_to_r(ctypes.byref(c), t_out, hits, 0, t_out, t_out + 64, None), "dr")
+    assert overlap(l.p2r_kalman_update(ctypes.byref(c), t_out, t_out + tb - 256, 0, None, None), "hits")
+    assert overlap(l.p2r_kalman_update(ctypes.byref(c), t_out, hits, 0, hits + lb, None), "chi2_accum")
+    h = np.zeros(tb + hb, np.uint8)  # host buffers are never dereferenced before the device checks
+    assert overlap(l.p2r_forward_host(ctypes.byref(c), h.ctypes.data, h.ctypes.data, h.ctypes.data, t_in, t_in + tb - 4,
+                                      t_out, 4, None), "dev_trk_in", "dev_hits")
+    assert overlap(l.p2r_forward_host(ctypes.byref(c), h.ctypes.data, h.ctypes.data, h.ctypes.data, t_in, hits,
+                                      hits + 4096, 4, None), "dev_hits", "dev_trk_out")
+    # adjacent ranges do not overlap. A call that passed every check would launch, so the
+    # boundary is shown with a launch shape that is rejected after the overlap checks.
+    bad_shape = _cfg(p2r, block_threads=100)
+    a_in, a_out, a_hit, a_chi2 = base, base + tb, base + 2 * tb, base + 2 * tb + hb  # end to end
+    assert l.p2r_forward(ctypes.byref(bad_shape), a_in, a_hit, a_out, a_chi2, None, None) == 1
+    assert "block_threads" in l.p2r_last_error_string().decode()
+    assert overlap(l.p2r_forward(ctypes.byref(bad_shape), a_in, a_hit, a_out - 4, None, None, None))
