@@ -89,7 +89,8 @@ float p2r_kfact(double bz);
  * &out->par) (TBB:656-812, called at TBB:894) for EVERY block b in [0, nevts*nb):
  * in = trk_in[b], hit = hits[layer + b*nlayer], out = trk_out[b]. trk_out's q is copied
  * from trk_in. trk_in may equal trk_out (the chained drivers' in-place call,
- * cuda_v4.cu:843). dr (nullable, nlayer floats) adds dr[layer] cm to the target radius. */
+ * cuda_v4.cu:843), but may not partly overlap it; trk_out may not overlap hits or dr.
+ * dr (nullable, nlayer floats) adds dr[layer] cm to the target radius. */
 int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hits, int32_t layer,
                        void* trk_out, const float* dr, void* stream);
 
@@ -97,14 +98,15 @@ int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hi
  * (TBB:433-642, called at TBB:911) for every block b: trk[b] updated in place with
  * hits[layer + b*nlayer]. chi2_accum (nullable, one float per track, track index
  * b*bsize + lane) gets the update's chi2 added (the reference's commented-out
- * Chi2Similarity, TBB:631). */
+ * Chi2Similarity, TBB:631). trk, hits and chi2_accum may not overlap. */
 int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_t layer, float* chi2_accum,
                       void* stream);
 
 /* ---------------------------------------------------------------- fused driver
  * The whole driver loop (TBB:873-926 for one iteration) in one launch: every track runs
  * all nlayer (propagate, update) pairs with its state in registers, reading each hit once.
- * trk_out may not alias trk_in. chi2_out (nullable) receives the summed chi2 per track.
+ * trk_out may not alias or overlap trk_in, and no written array (trk_out, chi2_out) may
+ * overlap any other array of the call. chi2_out (nullable) receives the summed chi2 per track.
  * dr (nullable, nlayer floats) as in p2r_propagate_to_r. In RESTART mode only the last
  * layer determines the result (TBB:894 overwrites the output each layer), and only that
  * layer is computed. */
@@ -135,7 +137,7 @@ int p2r_count_nonfinite(const void* trk, int64_t nblocks, int32_t bsize, unsigne
  * streams are shared), and the caller's stream waits for everything queued, also when a step
  * fails and an error is returned. In restart mode only the last layer's hit blocks are copied
  * (the only layer whose result reaches the output); the other layers' part of dev_hits is left
- * as it was. */
+ * as it was. The three device arrays may not overlap. */
 int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void* host_hits, void* host_trk_out,
                      void* dev_trk_in, void* dev_hits, void* dev_trk_out, int32_t nchunks, void* stream);
 
