@@ -241,14 +241,15 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import p2r_tests_b200 as p2r
+    # This arm maps no library of this package: the inputs come from the oracle's copy of the
+    # workload generator (bit-identical to p2r_gen_helix), the timed loop is the reference's.
     nthreads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    from oracle.oracle import ref_available, host_isa
+    from oracle.oracle import ref_available, host_isa, gen_helix
     if not ref_available(args.bsize, host_isa()):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref missing"}))
         return 0
     nb = NTRKS // args.bsize
-    cfg, trk, hit = make_inputs(p2r, args.nevts, args.bsize, 20240001)
+    trk, hit = gen_helix(args.bsize, args.nevts, nb, NLAYER, seed=20240001, bz=BZ)
     trk, hit = trk.reshape(-1), hit.reshape(-1)
     from oracle.oracle import RefTBB
     ref = RefTBB(args.bsize, host_isa())
@@ -281,9 +282,24 @@ def run_reference_arm(args):
         "cpu_baseline": {"value": value, "unit": "track-layer updates/s", "cores": nthreads,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "track-layer updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "mapped_libraries": mapped_in_tree_libraries(),
     }
     print(json.dumps(line))
     return 0
+
+
+def mapped_in_tree_libraries() -> list[str]:
+    """Shared libraries under this directory mapped into the process (from /proc/self/maps)."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and path.startswith(str(ROOT)):
+                    found.add(os.path.relpath(path, ROOT))
+    except OSError:
+        return []
+    return sorted(found)
 
 
 def workload_config(args):

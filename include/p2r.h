@@ -151,7 +151,9 @@ int p2r_forward_host(const p2r_config* cfg, const void* host_trk_in, const void*
  * by a persistent grid with one atomic counter; no thread waits on another.
  * The items and event offsets are device data and are not re-read on the host: each item
  * must cover blocks [block0, block0 + nblk) inside [0, nblocks) and inside its event's range,
- * which p2r_queue_plan guarantees for non-decreasing offsets from 0 to nblocks. Layer counts
+ * which p2r_queue_plan guarantees for non-decreasing offsets from 0 to nblocks. The kernels
+ * check every item and offset on the device before using it: a bad item is skipped (its event
+ * never completes) and recorded in the workspace, which p2r_queue_error reports. Layer counts
  * are clamped to [0, nlayer] on the device. */
 typedef struct p2r_queue_item {
   int32_t event; /* event of the range */
@@ -183,6 +185,13 @@ int64_t p2r_queue_plan(const int64_t* host_event_block_offset, int64_t nevts, in
 
 /* Device workspace for p2r_run_queue (item counter, per-event slice counters). */
 size_t p2r_queue_workspace_size(const p2r_queue* q);
+
+/* After a p2r_run_queue (or graph launch) on `stream` with this workspace: synchronises the
+ * stream and returns P2R_ERR_QUEUE if the device skipped malformed work items or event offsets
+ * (host_bits receives the reasons: 1 event outside [0, nevts), 2 blocks outside [0, nblocks),
+ * 4 blocks outside the item's event range, 8 event offsets decreasing or outside [0, nblocks]),
+ * P2R_OK otherwise. */
+int p2r_queue_error(const void* workspace, uint32_t* host_bits, void* stream);
 
 /* One persistent launch over all items (plus a small initialisation kernel). chi2_out
  * (nullable) per lane; event_done_ns (nullable, nevts) receives the %globaltimer value at
@@ -243,9 +252,11 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
  * captures a CUDA graph, event loops that forbid allocation after start-up, plugin hosts whose
  * device memory belongs to the host framework's pool. Batches whose workspace
  * (p2r_forward_backward_workspace_size) exceeds 8 MiB are rejected with P2R_ERR_WORKSPACE
- * (about 3 M tracks at 20 layers, fewer with more layers or events). The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress, with that device
- * current); make that first call before any stream capture. Every call shares the array:
+ * (about 3 M tracks at 20 layers, fewer with more layers or events). The array has its own
+ * address in every CUDA context (each device's primary context, and any context a plugin
+ * host creates and makes current): the first call in each context looks that address up
+ * (cudaGetSymbolAddress, with the context current) and caches it under the context's unique
+ * id; make that first call before any stream capture. Every call shares the array:
  * calls that overlap on the GPU race. Nothing in it needs clearing (each call writes
  * everything it reads). No cudaMalloc / cudaFree. */
 int p2r_forward_backward_noalloc(const p2r_config* cfg, const void* trk_in, const void* hits, const float* dr,

@@ -6,6 +6,8 @@ the product package.
 
   Oracle      the project's own CPU restatement (p2r_oracle.cpp), float and double
   RefTBB      the reference's CPU path compiled unmodified (ref_harness.cpp -> _ref/)
+  gen_helix   the benchmark's synthetic helix inputs (helix_gen.cpp), for the timed
+              reference arm, which must map no library of the product
 """
 from __future__ import annotations
 
@@ -72,6 +74,40 @@ class Oracle:
         chi2 = self.l.orc_step_f64(par.ctypes.data, cov.ctypes.data, int(q), hp.ctypes.data, hc.ctypes.data,
                                    float(dr), float(bz), po.ctypes.data, co.ctypes.data)
         return po, co, chi2
+
+
+# The benchmark workload's generator settings: the defaults of the product's p2r_gen_params
+# (include/p2r.h), in its field order after the seed.
+HELIX_DEFAULTS = {"seed": 20240001, "bz": 3.8, "r_seed": 15.0, "r_first": 20.0, "r_last": 100.0, "pt": 4.0,
+                  "pop_smear": 0.10, "theta_min": 0.3, "theta_max": 2.8, "cov_pos": 1e-4, "cov_ang": 1e-3,
+                  "est_smear": 1.0, "hit_sigma": 1e-3}
+
+
+def gen_helix(bsize: int, nevts: int, nb: int, nlayer: int, ntrk_event=None, nthreads: int = 0, **kw):
+    """Synthetic helix events (helix_gen.cpp), bit-identical to the product's p2r_gen_helix for
+    the same settings: returns host float32 (tracks, hits) shaped (nblocks, 28, bsize) and
+    (nblocks*nlayer, 9, bsize). Keyword arguments override HELIX_DEFAULTS."""
+    prm = dict(HELIX_DEFAULTS)
+    for k, v in kw.items():
+        if k not in prm:
+            raise KeyError(k)
+        prm[k] = v
+    lib = ctypes.CDLL(str(ORACLE_LIB))
+    fn = lib.orc_gen_helix
+    fn.argtypes = [ctypes.c_uint64, _vp, ctypes.c_int, ctypes.c_long, ctypes.c_long, ctypes.c_int, _vp, _vp, _vp,
+                   ctypes.c_int]
+    fn.restype = ctypes.c_int
+    vals = np.array([prm[k] for k in list(HELIX_DEFAULTS)[1:]], np.float64)
+    nblocks = nevts * nb
+    trk = np.empty((nblocks, 28, bsize), np.float32)
+    hit = np.empty((nblocks * nlayer, 9, bsize), np.float32)
+    nte = None if ntrk_event is None else np.ascontiguousarray(ntrk_event, np.int32)
+    if nte is not None and nte.shape != (nevts,):
+        raise ValueError("ntrk_event needs one entry per event")
+    if fn(prm["seed"], vals.ctypes.data, bsize, nevts, nb, nlayer, _p(nte), trk.ctypes.data, hit.ctypes.data,
+          nthreads) != 0:
+        raise ValueError("orc_gen_helix: bad sizes or geometry")
+    return trk, hit
 
 
 def host_isa() -> str:

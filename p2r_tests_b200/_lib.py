@@ -124,6 +124,7 @@ SIGNATURES = {
     "p2r_queue_plan": (ctypes.c_int64, [_vp, _i64, _i32, _vp, _i64]),
     "p2r_autotune_forward": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _i32, _vp, _i32, _i32, _vp, _vp]),
     "p2r_queue_workspace_size": (ctypes.c_size_t, [_vp]),
+    "p2r_queue_error": (ctypes.c_int, [_vp, _vp, _vp]),
     "p2r_run_queue": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "p2r_queue_graph_create": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "p2r_graph_launch": (ctypes.c_int, [_vp, _vp]),

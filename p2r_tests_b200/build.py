@@ -106,14 +106,18 @@ def build_driver(force: bool = False) -> Path:
 
 
 def build_oracle() -> None:
-    """Builds oracle/_build (always) and oracle/_ref (only where the reference checkout exists)."""
+    """Builds oracle/_build (always) and oracle/_ref from the reference checkout named by the
+    P2R_REFDIR environment variable (skipped when it is unset; an existing oracle/_ref is kept)."""
     make = shutil.which("make")
     if make is None:
         raise RuntimeError("make not found")
     subprocess.run([make, "-s", "-C", str(ROOT / "oracle"), "oracle"], check=True)
-    refdir = Path(os.environ.get("P2R_REFDIR", "/root/reference"))
-    if (refdir / "src" / "propagate-tor-test_tbb.cpp").exists():
-        subprocess.run([make, "-s", "-C", str(ROOT / "oracle"), "ref", f"REFDIR={refdir}"], check=True)
+    refdir = os.environ.get("P2R_REFDIR")
+    if not refdir:
+        return
+    if not (Path(refdir) / "src" / "propagate-tor-test_tbb.cpp").exists():
+        raise RuntimeError(f"P2R_REFDIR={refdir} holds no src/propagate-tor-test_tbb.cpp")
+    subprocess.run([make, "-s", "-C", str(ROOT / "oracle"), "ref", f"REFDIR={refdir}"], check=True)
 
 
 if __name__ == "__main__":

@@ -635,6 +635,31 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   if (!workspace || workspace_bytes < w.total_bytes)
     return p2r_set_errorf(P2R_ERR_WORKSPACE, "%s: workspace of %zu bytes needed", who, w.total_bytes);
   if (((uintptr_t)workspace & 255u) != 0) return p2r_set_errorf(P2R_ERR_INVALID, "%s: workspace must be 256-byte aligned", who);
+  {
+    // no written array may share a byte with another array of the call (the kernels read
+    // inputs after other tracks' outputs are written)
+    const size_t tb = (size_t)nblocks * 28 * cfg->bsize * sizeof(float);
+    const size_t hb = (size_t)nblocks * cfg->nlayer * 9 * cfg->bsize * sizeof(float);
+    const size_t lb = (size_t)nblocks * cfg->bsize * sizeof(float);
+    const size_t nl = (size_t)cfg->nlayer;
+    if ((rc = p2r_check_spans(
+             who, {{"trk_in", trk_in, tb, false},
+                   {"hits", hits, hb, false},
+                   {"dr", dr, nl * sizeof(float), false},
+                   {"nlay_lane", nlay_lane, lb, false},
+                   {"grad_trk_out", grad_trk_out, tb, false},
+                   {"grad_chi2", grad_chi2, lb, false},
+                   {"trk_out", trk_out, tb, true},
+                   {"chi2_out", chi2_out, lb, true},
+                   {"grad_trk_in", grad_trk_in, tb, true},
+                   {"grad_hits", grad_hits, hb, true},
+                   {"grad_dr", grad_dr, nl * sizeof(double), true},
+                   {"grad_bz", grad_bz, sizeof(double), true},
+                   {"grad_dr_event", grad_dr_event, (size_t)cfg->nevts * nl * sizeof(double), true},
+                   {"grad_bz_event", grad_bz_event, (size_t)cfg->nevts * sizeof(double), true},
+                   {"workspace", workspace, workspace_bytes, true}})))
+      return rc;
+  }
   AdjParams p;
   p.trk_in = (const float*)trk_in;
   p.hits = (const float*)hits;
@@ -702,6 +727,8 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
 // memory is entirely owned by the host framework's pool. For them the workspace of
 // p2r_forward_backward lives in this fixed device array instead. Every GPU that loads the
 // library holds the array until the process exits.
+#include <cuda.h>  // driver-API types only; the functions are reached through the runtime
+
 #include <mutex>
 
 namespace {
@@ -709,30 +736,76 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB per GPU
 static __device__ __align__(256) unsigned char g_fwdbwd_scratch[kNoAllocScratchBytes];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_scratch_mu;
-void* g_scratch_ptr[kNoAllocMaxDevices] = {};
+// The array has its own address in every CUDA context: the runtime's primary context of
+// each device, and any context a plugin host creates with the driver API and makes current.
+// The address is therefore cached per context, keyed by the context's process-unique id
+// (cuCtxGetId), so a context created after another was destroyed (cudaDeviceReset, a
+// host's own cuCtxDestroy / cuCtxCreate) never sees a stale address.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
 
-// Device address of g_fwdbwd_scratch on the current device. In host code the array's name
-// is only a host-side stand-in, so the address is looked up once per device (with that
-// device current) and cached.
+struct ScratchCache {
+  std::mutex mu;
+  bool resolved = false;
+  CtxGetCurrentFn ctx_current = nullptr;
+  CtxGetIdFn ctx_id = nullptr;
+  static constexpr int kSlots = 64;
+  unsigned long long ids[kSlots] = {};
+  void* ptrs[kSlots] = {};
+  int used = 0;
+};
+ScratchCache g_scratch;
+
+void resolve_driver_entry_points(ScratchCache& c) {
+  if (c.resolved) return;
+  c.resolved = true;
+  void* f = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    c.ctx_current = (CtxGetCurrentFn)f;
+  f = nullptr;
+  if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    c.ctx_id = (CtxGetIdFn)f;
+  cudaGetLastError();  // a failed query leaves no sticky error for the caller's next check
+}
+
+// Unique id of the calling thread's current context, or 0 if none is current (or the driver
+// cannot say).
+unsigned long long current_context_id(const ScratchCache& c) {
+  if (!c.ctx_current || !c.ctx_id) return 0;
+  CUcontext ctx = nullptr;
+  if (c.ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  unsigned long long id = 0;
+  return c.ctx_id(ctx, &id) == CUDA_SUCCESS ? id : 0;
+}
+
+// Device address of g_fwdbwd_scratch in the current context. In host code the array's name
+// is only a host-side stand-in, so its address is looked up with cudaGetSymbolAddress, with
+// the caller's context current, on the first call in each context, and cached.
 int scratch_address(void** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess)
-    return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_backward_noalloc: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= kNoAllocMaxDevices)
-    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "p2r_forward_backward_noalloc: device %d", dev);
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_fwdbwd_scratch);
-    if (e != cudaSuccess || !p)
-      return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_backward_noalloc: scratch address: %s",
-                            cudaGetErrorString(e));
-    g_scratch_ptr[dev] = p;
+  std::lock_guard<std::mutex> lk(g_scratch.mu);
+  resolve_driver_entry_points(g_scratch);
+  unsigned long long id = current_context_id(g_scratch);
+  if (id != 0)
+    for (int i = 0; i < g_scratch.used; ++i)
+      if (g_scratch.ids[i] == id) {
+        *out = g_scratch.ptrs[i];
+        return P2R_OK;
+      }
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_fwdbwd_scratch);
+  if (e != cudaSuccess || !p)
+    return p2r_set_errorf(P2R_ERR_CUDA, "p2r_forward_backward_noalloc: scratch address: %s", cudaGetErrorString(e));
+  // the lookup makes the device's primary context current if no context was
+  if (id == 0) id = current_context_id(g_scratch);
+  if (id != 0 && g_scratch.used < ScratchCache::kSlots) {  // otherwise: looked up again on every call
+    g_scratch.ids[g_scratch.used] = id;
+    g_scratch.ptrs[g_scratch.used] = p;
+    ++g_scratch.used;
   }
-  *out = g_scratch_ptr[dev];
+  *out = p;
   return P2R_OK;
 }
 

@@ -54,6 +54,20 @@ int p2r_check_disjoint(const char* who, const char* what, const void* a, size_t 
   return P2R_OK;
 }
 
+int p2r_check_spans(const char* who, std::initializer_list<P2rSpan> spans) {
+  const P2rSpan* v = spans.begin();
+  const size_t n = spans.size();
+  for (size_t i = 0; i < n; ++i)
+    for (size_t j = i + 1; j < n; ++j) {
+      if (!v[i].written && !v[j].written) continue;
+      if (!v[i].ptr || !v[j].ptr || v[i].bytes == 0 || v[j].bytes == 0) continue;
+      const uintptr_t a = (uintptr_t)v[i].ptr, b = (uintptr_t)v[j].ptr;
+      if (a < b + v[j].bytes && b < a + v[i].bytes)
+        return p2r_set_errorf(P2R_ERR_INVALID, "%s: %s and %s overlap", who, v[i].name, v[j].name);
+    }
+  return P2R_OK;
+}
+
 int p2r_check_config(const p2r_config* cfg, const char* who) {
   if (!cfg) return p2r_set_errorf(P2R_ERR_INVALID, "%s: config is null", who);
   if (cfg->bsize < 1 || cfg->bsize > 4096)

@@ -32,6 +32,19 @@ int p2r_check_aligned(const char* who, unsigned align, std::initializer_list<con
 int p2r_check_disjoint(const char* who, const char* what, const void* a, size_t na, const void* b, size_t nb,
                        bool allow_same = false);
 
+// One array argument of a launch: its name, first byte, size in bytes, and whether the launch
+// writes it.
+struct P2rSpan {
+  const char* name;
+  const void* ptr;
+  size_t bytes;
+  bool written;
+};
+
+// P2R_ERR_INVALID when a written array shares a byte with any other array of the same launch
+// (written or read), naming the pair. Null pointers and empty ranges overlap nothing.
+int p2r_check_spans(const char* who, std::initializer_list<P2rSpan> spans);
+
 // Names an entry point's span on a profiler's host timeline (an NVTX range: header-only, a
 // no-op unless a tool such as Nsight Systems or Nsight Compute is attached).
 struct P2rRange {

@@ -8,7 +8,9 @@
 // 32-lane slices of the item's blocks and runs them with the chained staged body of the
 // fused forward. When the last slice of an event finishes, its warp records %globaltimer
 // into event_done_ns[event], giving per-event completion times. No thread waits on another
-// (items are claimed with one atomicAdd), so there is no spin loop to bound.
+// (items are claimed with one atomicAdd), so there is no spin loop to bound. Items and event
+// offsets are device data: each is range-checked on the device before use, and a bad one is
+// skipped and recorded in an error word of the workspace (read by p2r_queue_error).
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -26,6 +28,9 @@ struct QueueParams {
   long long n_items;
   int* counter;                 // next item
   int* ev_remaining;            // slices left per event
+  const int64_t* ev_off;        // event block offsets (nevts + 1)
+  long long nevts;
+  unsigned* error;              // P2R_QERR_* bits of items that were skipped
   unsigned long long* ev_done;  // nullable
   unsigned long long* t_start;  // nullable
 };
@@ -36,13 +41,28 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 
-__global__ void queue_init_kernel(const int64_t* ev_off, long long nevts, int slices_per_block, int* counter,
-                                  int* ev_remaining, unsigned long long* t_start) {
+// Error bits of the queue's device-side checks (the word p2r_queue_error reads).
+constexpr unsigned kQerrEvent = 1u;       // an item's event outside [0, nevts)
+constexpr unsigned kQerrBlocks = 2u;      // an item's blocks outside [0, nblocks) or nblk < 0
+constexpr unsigned kQerrEventRange = 4u;  // an item's blocks outside its event's block range
+constexpr unsigned kQerrOffsets = 8u;     // event offsets decreasing, outside [0, nblocks], or too large
+
+__global__ void queue_init_kernel(const int64_t* ev_off, long long nevts, long long nblocks, int slices_per_block,
+                                  int* counter, int* ev_remaining, unsigned* error, unsigned long long* t_start) {
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < nevts) ev_remaining[e] = (int)((ev_off[e + 1] - ev_off[e]) * slices_per_block);
   if (e == 0) {
     *counter = 0;
     if (t_start) *t_start = ULLONG_MAX;
+  }
+  if (e < nevts) {
+    const long long b0 = ev_off[e], b1 = ev_off[e + 1];
+    const long long n = (b1 - b0) * slices_per_block;
+    if (b0 < 0 || b1 < b0 || b1 > nblocks || n > INT_MAX) {
+      atomicOr(error, kQerrOffsets);
+      ev_remaining[e] = 0;
+    } else {
+      ev_remaining[e] = (int)n;
+    }
   }
 }
 
@@ -62,6 +82,20 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
     __syncthreads();  // every thread has read s_item before thread 0 claims the next one
     if (item >= q.n_items) break;
     const p2r_queue_item qi = q.items[item];
+    // the items are device data the host did not re-read: an item outside the arrays is
+    // skipped and reported (p2r_queue_error), never indexed
+    unsigned bad = 0u;
+    if (qi.event < 0 || qi.event >= q.nevts) {
+      bad = kQerrEvent;
+    } else if (qi.nblk < 0 || qi.block0 < 0 || qi.block0 > q.f.nblocks - qi.nblk) {
+      bad = kQerrBlocks;
+    } else if (qi.block0 < q.ev_off[qi.event] || qi.block0 + qi.nblk > q.ev_off[qi.event + 1]) {
+      bad = kQerrEventRange;
+    }
+    if (bad) {
+      if (threadIdx.x == 0) atomicOr(q.error, bad);
+      continue;
+    }
     const int nslices = qi.nblk * spb;
     for (int s = warp; s < nslices; s += nwarps) {
       const long long b = qi.block0 + s / spb;
@@ -108,12 +142,13 @@ using namespace p2r;
 namespace {
 
 struct QueueWs {
-  size_t counter_off, start_off, remaining_off, bytes;
+  size_t counter_off, error_off, start_off, remaining_off, bytes;
 };
 
 QueueWs queue_ws(int64_t nevts) {
   QueueWs w;
   w.counter_off = 0;
+  w.error_off = 128;
   w.start_off = 256;
   w.remaining_off = 512;
   w.bytes = 512 + (((size_t)nevts * sizeof(int) + 255) & ~(size_t)255);
@@ -156,6 +191,24 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
   if ((rc = p2r_check_aligned(who, 4, {trk_in, trk_out, chi2_out, q->nlay_lane})) ||
       (rc = p2r_check_aligned(who, 8, {event_done_ns, start_ns, q->event_block_offset, q->items})))
     return rc;
+  {
+    const size_t tb = (size_t)q->nblocks * 28 * q->bsize * sizeof(float);
+    const size_t hb = (size_t)q->nblocks * q->nlayer * 9 * q->bsize * sizeof(float);
+    const size_t lb = (size_t)q->nblocks * q->bsize * sizeof(float);
+    const size_t ne = (size_t)q->nevts;
+    if ((rc = p2r_check_spans(
+             who, {{"trk_in", trk_in, tb, false},
+                   {"hits", hits, hb, false},
+                   {"nlay_lane", q->nlay_lane, lb, false},
+                   {"event_block_offset", q->event_block_offset, (ne + 1) * sizeof(int64_t), false},
+                   {"items", q->items, (size_t)q->n_items * sizeof(p2r_queue_item), false},
+                   {"trk_out", trk_out, tb, true},
+                   {"chi2_out", chi2_out, lb, true},
+                   {"event_done_ns", event_done_ns, ne * sizeof(unsigned long long), true},
+                   {"start_ns", start_ns, sizeof(unsigned long long), true},
+                   {"workspace", workspace, ws_bytes, true}})))
+      return rc;
+  }
   QueueParams qp;
   qp.f.trk_in = (const float*)trk_in;
   qp.f.hits = (const float*)hits;
@@ -173,10 +226,16 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
   qp.counter = (int*)((char*)workspace + w.counter_off);
   qp.t_start = start_ns;
   qp.ev_remaining = (int*)((char*)workspace + w.remaining_off);
+  qp.ev_off = q->event_block_offset;
+  qp.nevts = q->nevts;
+  qp.error = (unsigned*)((char*)workspace + w.error_off);
   qp.ev_done = event_done_ns;
+  // the error word is cleared before any kernel of this launch can set a bit
+  cudaError_t e = cudaMemsetAsync(qp.error, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
   queue_init_kernel<<<(unsigned)((q->nevts + 255) / 256), 256, 0, st>>>(
-      q->event_block_offset, q->nevts, q->bsize / 32, qp.counter, qp.ev_remaining, start_ns);
-  cudaError_t e = cudaGetLastError();
+      q->event_block_offset, q->nevts, q->nblocks, q->bsize / 32, qp.counter, qp.ev_remaining, qp.error, start_ns);
+  e = cudaGetLastError();
   if (e == cudaSuccess) {
     const int threads = q->block_threads > 0 ? q->block_threads : 128;
     const int stages = q->stages > 0 ? q->stages : 4;
@@ -240,6 +299,25 @@ int64_t p2r_queue_plan(const int64_t* host_event_block_offset, int64_t nevts, in
 size_t p2r_queue_workspace_size(const p2r_queue* q) {
   if (!q || q->nevts < 0) return 0;
   return queue_ws(q->nevts).bytes;
+}
+
+int p2r_queue_error(const void* workspace, uint32_t* host_bits, void* stream) {
+  if (!workspace || !host_bits) return p2r_set_error(P2R_ERR_INVALID, "p2r_queue_error: null pointer");
+  if (((uintptr_t)workspace & 255u) != 0)
+    return p2r_set_error(P2R_ERR_INVALID, "p2r_queue_error: workspace must be 256-byte aligned");
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned bits = 0u;
+  cudaError_t e = cudaMemcpyAsync(&bits, (const char*)workspace + queue_ws(0).error_off, sizeof(bits),
+                                  cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "p2r_queue_error: %s", cudaGetErrorString(e));
+  *host_bits = bits;
+  if (bits)
+    return p2r_set_errorf(P2R_ERR_QUEUE,
+                          "p2r_queue_error: work items were skipped (bits 0x%x: 1 event out of range, 2 blocks out "
+                          "of range, 4 blocks outside the event's range, 8 bad event offsets)",
+                          bits);
+  return p2r_clear_error();
 }
 
 int p2r_run_queue(const p2r_queue* q, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,

@@ -196,6 +196,15 @@ class Queue:
             lib().p2r_graph_destroy(self.graph)
             self.graph = None
 
+    def error_bits(self, stream=None) -> int:
+        """Synchronises `stream` and returns the device-side check bits of the last launch
+        (0: every work item and event offset was in range; see p2r_queue_error)."""
+        bits = ctypes.c_uint32(0)
+        rc = lib().p2r_queue_error(_ptr(self.ws), ctypes.byref(bits), _stream(stream))
+        if rc not in (_lib.P2R_OK, _lib.P2R_ERR_QUEUE):
+            check(rc)
+        return int(bits.value)
+
     def event_latency_ns(self) -> np.ndarray:
         """Per-event completion time relative to the earliest CTA start of the last launch."""
         return (self.done_ns - self.start_ns).cpu().numpy()

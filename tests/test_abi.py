@@ -233,3 +233,73 @@ def test_overlapping_arrays_rejected(p2r):
     assert l.p2r_forward(ctypes.byref(bad_shape), a_in, a_hit, a_out, a_chi2, None, None) == 1
     assert "block_threads" in l.p2r_last_error_string().decode()
     assert overlap(l.p2r_forward(ctypes.byref(bad_shape), a_in, a_hit, a_out - 4, None, None, None))
+
+
+@pytest.mark.usefixtures("host_only")
+def test_adjoint_overlapping_arrays_rejected(p2r):
+    """p2r_forward_backward (and so its allocation-free variant): no written array (outputs,
+    gradients, workspace) may share a byte with another array of the call. Fake addresses,
+    compared on the host only."""
+    l = p2r.lib()
+    c = _cfg(p2r)  # one block of 32 tracks, 20 layers
+    c.mode = p2r.MODE_CHAINED
+    tb, hb, lb = 28 * 32 * 4, 20 * 9 * 32 * 4, 32 * 4
+    need = l.p2r_forward_backward_workspace_size(ctypes.byref(c))
+    base = 1 << 33
+    a = {n: base + i * (1 << 20) for i, n in enumerate(
+        ("trk_in", "hits", "dr", "nlay", "trk_out", "chi2", "g_out", "g_chi2", "g_in", "g_hits", "g_dr", "g_bz",
+         "g_dr_ev", "g_bz_ev", "ws"))}
+
+    def call(**over):
+        v = {**a, **over}
+        return l.p2r_forward_backward(ctypes.byref(c), v["trk_in"], v["hits"], v["dr"], v["nlay"], v["trk_out"],
+                                      v["chi2"], v["g_out"], v["g_chi2"], v["g_in"], v["g_hits"], v["g_dr"],
+                                      v["g_bz"], v["g_dr_ev"], v["g_bz_ev"], 5, v["ws"], need, None)
+
+    def overlap(rc, *words):
+        msg = l.p2r_last_error_string().decode()
+        return rc == 1 and "overlap" in msg and all(w in msg for w in words)
+
+    assert overlap(call(trk_out=a["trk_in"] + 256), "trk_in", "trk_out")
+    assert overlap(call(g_in=a["hits"] + hb - 4), "hits", "grad_trk_in")
+    assert overlap(call(g_hits=a["trk_out"] + tb - 8), "trk_out", "grad_hits")
+    assert overlap(call(chi2=a["g_chi2"]), "grad_chi2", "chi2_out")
+    assert overlap(call(g_dr=a["dr"]), "dr", "grad_dr")
+    assert overlap(call(g_bz=a["g_dr"] + 8 * 19), "grad_dr", "grad_bz")
+    assert overlap(call(g_bz_ev=a["g_dr_ev"]), "grad_dr_event", "grad_bz_event")
+    assert overlap(call(ws=a["g_out"]), "grad_trk_out", "workspace")
+    assert overlap(call(nlay=a["chi2"] + lb - 4), "nlay_lane", "chi2_out")
+    # two read-only arrays may share memory (the same hits passed twice is harmless) ...
+    assert not overlap(call(g_out=a["trk_in"], trk_in=a["trk_in"], ws=a["ws"] + 1))
+    # ... that call was rejected by the workspace alignment check after the overlap checks
+    assert "256-byte" in l.p2r_last_error_string().decode()
+
+
+@pytest.mark.usefixtures("host_only")
+def test_queue_overlapping_arrays_rejected(p2r):
+    """p2r_run_queue: outputs, timestamps and workspace may not overlap any array of the call."""
+    from p2r_tests_b200._lib import CQueue
+    l = p2r.lib()
+    base = 1 << 34
+    off, items, nlay = base, base + (1 << 20), base + (2 << 20)
+    t_in, hits, t_out = base + (3 << 20), base + (4 << 20), base + (5 << 20)
+    chi2, done, start, ws = base + (6 << 20), base + (7 << 20), base + (8 << 20), base + (9 << 20)
+    q = CQueue(32, 20, 2, 2, 3.8, 0, 0, 0, 0, off, items, 2, nlay)
+    need = l.p2r_queue_workspace_size(ctypes.byref(q))
+
+    def call(**over):
+        v = dict(t_in=t_in, hits=hits, t_out=t_out, chi2=chi2, done=done, start=start, ws=ws)
+        v.update(over)
+        return l.p2r_run_queue(ctypes.byref(q), v["t_in"], v["hits"], v["t_out"], v["chi2"], v["done"], v["start"],
+                               v["ws"], need, None)
+
+    def overlap(rc, *words):
+        msg = l.p2r_last_error_string().decode()
+        return rc == 1 and "overlap" in msg and all(w in msg for w in words)
+
+    assert overlap(call(t_out=t_in + 64), "trk_in", "trk_out")
+    assert overlap(call(chi2=nlay), "nlay_lane", "chi2_out")
+    assert overlap(call(done=items), "items", "event_done_ns")
+    assert overlap(call(start=off + 8), "event_block_offset", "start_ns")
+    assert overlap(call(ws=t_out + 256), "trk_out", "workspace")
+    assert overlap(call(ws=hits), "hits", "workspace")

@@ -28,6 +28,33 @@ def fixture_inputs(p2r, golden_dir, bs):
     return cfg, trk, hit, g
 
 
+@pytest.mark.parametrize("bs,nevts,nlayer,seed,bz,ntrk_event", [
+    (32, 2, 20, 20240001, 3.8, None),        # the benchmark workload's seed (9600 tracks per event)
+    (32, 2, 20, 20240000, 3.8, None),        # the 10-event workload's seed
+    (64, 2, 20, 20240002, 3.8, None),
+    (32, 3, 40, 20240004, 3.8, [9600, 50, 777]),  # uneven events, 40 layers
+    (128, 2, 25, 11, -2.0, [100, 9600]),     # reversed field
+])
+def test_oracle_helix_generator_bit_identical(p2r, bs, nevts, nlayer, seed, bz, ntrk_event):
+    """The oracle's generator (used by the timed reference arm, which maps no product library)
+    writes the same inputs as the product's p2r_gen_helix, bit for bit."""
+    from oracle.oracle import gen_helix
+    nb = 9600 // bs
+    cfg = p2r.Config(bsize=bs, nlayer=nlayer, nevts=nevts, nb=nb, bz=bz)
+    a_trk, a_hit = p2r.generate_helix(cfg, p2r.gen_params(bz=bz, seed=seed), ntrk_event=ntrk_event)
+    b_trk, b_hit = gen_helix(bs, nevts, nb, nlayer, ntrk_event=ntrk_event, seed=seed, bz=bz)
+    assert np.array_equal(a_trk.view(np.uint32), b_trk.view(np.uint32))
+    assert np.array_equal(a_hit.view(np.uint32), b_hit.view(np.uint32))
+
+
+def test_oracle_helix_defaults_match_product(p2r):
+    """The oracle generator's default settings are the product's p2r_gen_params defaults."""
+    from oracle.oracle import HELIX_DEFAULTS
+    gp = p2r.gen_params()
+    for k, v in HELIX_DEFAULTS.items():
+        assert getattr(gp, k) == v, k
+
+
 @pytest.mark.parametrize("bs", [32, 64, 128])
 def test_fixture_generator_bit_exact(p2r, golden_dir, bs):
     """p2r_gen_fixture reproduces the reference's prepareTracks/prepareHits (TBB:243-293) bit for bit."""

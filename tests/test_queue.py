@@ -208,3 +208,54 @@ def test_queue_wide_blocks(p2r, torch, bs):
     p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
     torch.cuda.synchronize()
     parity.assert_same_arithmetic(out.cpu().numpy(), ref.cpu().numpy(), bs, f"queue bsize {bs}")
+
+
+@pytest.mark.gpu
+def test_queue_skips_and_reports_malformed_items(p2r, torch, small_batch):
+    """Work items and event offsets are device data: the kernel range-checks each one before
+    use, skips a bad one and reports it (p2r_queue_error). Every buffer here is a real
+    allocation of the right size; the out-of-range values are only ever compared, never used
+    as an index (checked by reading the kernel). The good items' outputs are bit-identical to
+    the masked forward's, the bad items' blocks are left untouched."""
+    w = small_batch
+    q = p2r.Queue(w, blocks_per_item=2)
+    t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
+    out = torch.full_like(t, float("nan"))
+    q.run(t, h, out)
+    assert q.error_bits() == 0
+    items = q.d_items.cpu().numpy().view(np.dtype([("event", np.int32), ("nblk", np.int32), ("block0", np.int64)]))
+    bad = items.copy()
+    nev, nblocks = q.nevts, w["nblocks"]
+    bad[1]["event"] = nev + 3                       # event out of range
+    bad[2]["block0"] = nblocks + 5                  # blocks past the end
+    bad[3]["nblk"] = -1                             # negative count
+    off = w["event_block_offset"]
+    bad[4]["event"] = (int(bad[4]["event"]) + 1) % nev  # in range, but not the event owning its blocks
+    skipped = [1, 2, 3, 4]
+    q.d_items.copy_(torch.from_numpy(bad.view(np.uint8).copy()))
+    out2 = torch.full_like(t, float("nan"))
+    q.run(t, h, out2)
+    assert q.error_bits() == 1 | 2 | 4
+    ref = torch.empty_like(t)
+    cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"])
+    p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
+    torch.cuda.synchronize()
+    o2 = out2.cpu().numpy().reshape(nblocks, 28, 32)
+    r = ref.cpu().numpy().reshape(nblocks, 28, 32)
+    untouched = np.zeros(nblocks, bool)
+    for i in skipped:
+        b0, n = int(items[i]["block0"]), int(items[i]["nblk"])
+        untouched[b0:b0 + n] = True
+    assert np.isnan(o2[untouched]).all()
+    assert np.array_equal(o2[~untouched].view(np.uint32), r[~untouched].view(np.uint32))
+    # decreasing event offsets are reported too (their events' items still run in range)
+    q.d_items.copy_(torch.from_numpy(items.view(np.uint8).copy()))
+    d_off = q.d_off.clone()
+    o = off.copy()
+    o[1] = -1
+    q.d_off.copy_(torch.from_numpy(np.ascontiguousarray(o, np.int64)))
+    q.run(t, h, torch.empty_like(t))
+    assert q.error_bits() & 8
+    q.d_off.copy_(d_off)
+    q.run(t, h, torch.empty_like(t))
+    assert q.error_bits() == 0

@@ -77,11 +77,12 @@ def test_noalloc_matches_workspace_entry_point(p2r, torch):
 
 
 def test_noalloc_rejects_oversized_batch(p2r):
-    # the size check runs before any device work
+    # the size check runs before any device work; the arrays are null, so a call that got past
+    # it would be rejected by the workspace entry point's null-input check, never launched
     cfg = p2r.Config(bsize=32, nlayer=64, nevts=10, nb=4000, bz=3.8, mode=p2r.MODE_CHAINED)
     lib = p2r.lib()
     c = cfg.c()
-    rc = lib.p2r_forward_backward_noalloc(ctypes.byref(c), 16, 16, None, None, None, None, None, None, None, None,
-                                          None, None, None, None, 5, None)
+    rc = lib.p2r_forward_backward_noalloc(ctypes.byref(c), None, None, None, None, None, None, None, None, None,
+                                          None, None, None, None, None, 5, None)
     assert rc == p2r._lib.P2R_ERR_WORKSPACE
     assert "scratch" in lib.p2r_last_error_string().decode()
