@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--mode", choices=["chained", "restart"], default="chained")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's CUDA kernels")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=10)
     ap.add_argument("--no-sweep", action="store_true")
@@ -176,7 +177,7 @@ def measured_peaks():
 
 
 # ------------------------------------------------------------------ CPU reference timing
-def accuracy_vs_fp64(trk_ev, hit_ev, ours_ev, nb, bsize, bz, nthreads):
+def accuracy_vs_fp64(trk_ev, hit_ev, ours_ev, nb, bsize, bz, nthreads, ref_gpu_ev=None):
     """Error of this library's output and of the reference's own CPU output against the FP64
     oracle on one event of the bench workload (the oracle as the checker). Parameters:
     |a - f64| / max(|f64|, floor), floor (1, 1, 1, 0.01, 1, 1) for (x, y, z, 1/pT, phi, theta);
@@ -189,22 +190,96 @@ def accuracy_vs_fp64(trk_ev, hit_ev, ours_ev, nb, bsize, bz, nthreads):
     d = np.sqrt(np.abs(f64["prior"][:, diag]))
     scale = np.concatenate([d[:, i:i + 1] * d[:, :i + 1] for i in range(6)], axis=1)  # packed (i, j <= i)
 
-    def errs(out):
+    def unpack(out):
         t = np.ascontiguousarray(out, np.float32).reshape(-1, 28, bsize)
         par = t[:, 0:6, :].transpose(0, 2, 1).reshape(-1, 6).astype(np.float64)
         cov = t[:, 6:27, :].transpose(0, 2, 1).reshape(-1, 21).astype(np.float64)
-        ep = np.abs(par - f64["par"]) / np.maximum(np.abs(f64["par"]), floor)
-        ec = np.abs(cov - f64["cov"]) / np.maximum(np.abs(f64["cov"]), scale)
+        return par, cov
+
+    def errs(out, against=None):
+        """Quantiles of the relative errors of `out` against the FP64 oracle (or against another
+        output), and the fractions of elements beyond the stated bars (1e-4 parameters, 1e-3
+        covariance)."""
+        par, cov = unpack(out)
+        tp, tc = (f64["par"], f64["cov"]) if against is None else unpack(against)
+        ep = np.abs(par - tp) / np.maximum(np.abs(tp), floor)
+        ec = np.abs(cov - tc) / np.maximum(np.abs(tc), scale)
         q = lambda e: {"p50": float(np.quantile(e, 0.5)), "p99": float(np.quantile(e, 0.99)), "max": float(e.max())}
-        return {"par": q(ep), "cov": q(ec)}
+        return {"par": q(ep), "cov": q(ec), "frac_par_beyond_1e-4": float((ep > 1e-4).mean()),
+                "frac_cov_beyond_1e-3": float((ec > 1e-3).mean())}
 
     res = {"sample": f"event 0 of the bench workload ({nb * bsize} tracks x {NLAYER} layers, chained)",
-           "oracle": "own FP64 restatement (oracle/), Bz as the workload", "this_library": errs(ours_ev)}
+           "oracle": "own FP64 restatement (oracle/), Bz as the workload", "this_library": errs(ours_ev),
+           "bars": "fractions of elements beyond relative 1e-4 (parameters, floors 1 cm / 0.01 GeV^-1 / 1 rad) "
+                   "and 1e-3 (covariance, scale max(|C_ij|, sqrt(P_ii P_jj)) with P the covariance entering the "
+                   "last update)"}
     if ref_available(bsize, "kf"):
         ref = RefTBB(bsize, "kf")
         ref.set_bz(bz)
-        res["reference_cpu"] = errs(ref.run(trk_ev, hit_ev, 1, nb, NLAYER, True, 1, nthreads))
+        ref_out = ref.run(trk_ev, hit_ev, 1, nb, NLAYER, True, 1, nthreads)
+        res["reference_cpu"] = errs(ref_out)
+        res["this_library_vs_reference_cpu"] = errs(ours_ev, against=ref_out)
+    if ref_gpu_ev is not None:
+        res["reference_gpu_cuda_v4"] = errs(ref_gpu_ev)
     return res
+
+
+def reference_gpu(p2r, torch, cfg, d_trk, d_hit, stream, steps, ours_chained_ms):
+    """The reference's own CUDA kernels (compiled unmodified from its sources into oracle/_ref)
+    timed with CUDA events on the same device-resident inputs as this library's fused kernel:
+    GPUsequence (cuda_v4.cu:821-849, chained, against p2r_forward CHAINED) and launch_p2r_kernel
+    (cuda_uvm.cu:887-915, restart, against p2r_forward RESTART). Returns the record and the
+    chained kernel's output (for the accuracy comparison), or (None, None)."""
+    from oracle.oracle import RefGPU, refgpu_available
+    rec, out_v4 = {}, None
+    for kind in ("v4", "uvm"):
+        if not refgpu_available(kind):
+            rec[kind] = {"unavailable": "oracle/_ref/libp2r_refgpu_" + kind + ".so missing"}
+            continue
+        r = RefGPU(kind)
+        ne, nb, nl, bs = r.sizes()
+        if (ne, nb, nl, bs) != (cfg.nevts, cfg.nb, cfg.nlayer, cfg.bsize):
+            rec[kind] = {"unavailable": f"compiled for nevts={ne} nb={nb} nlayer={nl} bsize={bs}"}
+            continue
+        out = torch.empty_like(d_trk)
+        ms = r.run(d_trk.data_ptr(), d_hit.data_ptr(), out.data_ptr(), 3, steps, stream.cuda_stream) / steps
+        if r.chained:
+            ours = ours_chained_ms
+            out_v4 = out
+            what = ("GPUsequence, src/propagate-tor-test_cuda_v4.cu:821-849: chained layer loop, one 32-thread "
+                    "CTA per Matriplex block, scratch matrices in shared memory; against p2r_forward CHAINED")
+            ups = cfg.ntracks * cfg.nlayer
+        else:
+            rcfg = dataclasses.replace(cfg, mode=p2r.MODE_RESTART)
+            o2 = torch.empty_like(d_trk)
+            for _ in range(3):
+                p2r.forward(rcfg, d_trk, d_hit, o2, stream=stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                p2r.forward(rcfg, d_trk, d_hit, o2, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ours = e0.elapsed_time(e1) / steps
+            torch.cuda.synchronize()
+            same = torch.equal(torch.isfinite(out), torch.isfinite(o2))
+            del o2
+            what = ("launch_p2r_kernel, src/propagate-tor-test_cuda_uvm.cu:887-915: restart layer loop (every "
+                    "layer starts from the input track, only the last result is stored, so the compiler may "
+                    "drop the other layers), one thread per track; against p2r_forward RESTART (which computes "
+                    "only the last layer)")
+            ups = cfg.ntracks
+        rec[kind] = {"kernel": what, "ms_per_pass": ms, "this_library_ms_per_pass": ours,
+                     "speedup_of_this_library": ms / ours, "updates_per_s": ups / (ms / 1e3),
+                     "steps": steps,
+                     "build": "nvcc -gencode arch=compute_100a,code=sm_100a -std=c++17 -maxrregcount=64 -g -lineinfo "
+                              "--expt-relaxed-constexpr (the reference's build.py:97 flags, sm_100a for sm_70), "
+                              "-Dntrks=9600 -Dnevts=100 -Dnlayer=20 -Dbsize=32"}
+        if not r.chained:
+            rec[kind]["nonfinite_pattern_equal"] = bool(same)
+        else:
+            del out
+    return rec, out_v4
 
 
 def cpu_reference_rate(trk, hit, nevts, nb, bsize, budget_s, nthreads):
@@ -725,6 +800,15 @@ def main():
             "how": "one whole-buffer pinned cudaMemcpyAsync per direction (torch copy_), after the "
                    "end-to-end steps; frac = the end-to-end step's H2D bytes / its time, over h2d_gbs_measured"}
 
+    # the reference's own CUDA kernels on this GPU, same inputs (1-GPU runs of the default workload)
+    ref_gpu, ref_gpu_out = None, None
+    if world == 1 and not restart and not args.no_reference_gpu:
+        try:
+            ref_gpu, ref_gpu_out = reference_gpu(p2r, torch, cfg, d_trk, d_hit, stream, min(args.steps, 200),
+                                                 ms_per_step)
+        except Exception as exc:  # reported, not fatal
+            ref_gpu = {"unavailable": str(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not restart:  # timed on the chained loop
         try:
@@ -734,8 +818,9 @@ def main():
             cpu = {"value": v, "unit": "track-layer updates/s", "cores": thr, "kind": "reference",
                    "sample": sample + f"; reference build oracle/_ref ({kind}), Bz compiled in at 3.8112 T"}
             tw, hw = 28 * cfg.bsize * cfg.nb, 9 * cfg.bsize * cfg.nb * NLAYER
-            cpu["accuracy_vs_fp64"] = accuracy_vs_fp64(trk.reshape(-1)[:tw], hit.reshape(-1)[:hw],
-                                                       d_out[:tw].cpu().numpy(), cfg.nb, cfg.bsize, BZ, nthreads)
+            cpu["accuracy_vs_fp64"] = accuracy_vs_fp64(
+                trk.reshape(-1)[:tw], hit.reshape(-1)[:hw], d_out[:tw].cpu().numpy(), cfg.nb, cfg.bsize, BZ,
+                nthreads, None if ref_gpu_out is None else ref_gpu_out[:tw].cpu().numpy())
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "unit": "track-layer updates/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
@@ -769,6 +854,7 @@ def main():
             "bsize_sweep": sweep,
             "uneven_batch": uneven,
             "calibration_40_layers": calib,
+            "reference_gpu": ref_gpu,
             "gpu_launches": args.steps,
             "clocks": clk,
             "nonfinite_tracks": nonfinite,

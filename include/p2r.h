@@ -102,6 +102,22 @@ int p2r_propagate_to_r(const p2r_config* cfg, const void* trk_in, const void* hi
 int p2r_kalman_update(const p2r_config* cfg, void* trk, const void* hits, int32_t layer, float* chi2_accum,
                       void* stream);
 
+/* The reference's 3x3 gain routines, which it defines but never calls (its KalmanUpdate
+ * measures two coordinates and inverts a 2x2):
+ *   p2r_kalman_gain_inv replaces KalmanGainInv(&trk->cov, &hit->cov, &inv) (TBB:376-404) for
+ *     every block b, hit = hits[layer + b*nlayer], writing one MP3x3 block (9*bsize floats,
+ *     row-major 3x3 per lane) per track block to inv_out. Determinant and its reciprocal in
+ *     double, as TBB:383-388.
+ *   p2r_kalman_gain replaces KalmanGain(&trk->cov, &inv, &gain) (TBB:405-426), writing one
+ *     MP3x6 block (18*bsize floats, row-major 6x3 per lane) per track block to gain_out.
+ * Both read the packed covariances with the reference's own element choice: as if they were
+ * packed upper-triangle row-major, whereas the arrays are packed lower-triangle (TBB:46-54),
+ * so the 3x3 they invert is not the position block. The written array may not overlap the
+ * others. */
+int p2r_kalman_gain_inv(const p2r_config* cfg, const void* trk, const void* hits, int32_t layer, float* inv_out,
+                        void* stream);
+int p2r_kalman_gain(const p2r_config* cfg, const void* trk, const float* inv, float* gain_out, void* stream);
+
 /* ---------------------------------------------------------------- fused driver
  * The whole driver loop (TBB:873-926 for one iteration) in one launch: every track runs
  * all nlayer (propagate, update) pairs with its state in registers, reading each hit once.
@@ -264,6 +280,32 @@ int p2r_forward_backward_noalloc(const p2r_config* cfg, const void* trk_in, cons
                                  const float* grad_chi2, void* grad_trk_in, void* grad_hits, double* grad_dr,
                                  double* grad_bz, double* grad_dr_event, double* grad_bz_event, int32_t ckpt_stride,
                                  void* stream);
+
+/* Fused forward + adjoint of an uneven batch in ONE persistent launch over the work queue
+ * (no counterpart in the reference): the batch, its events, work items and per-lane layer
+ * counts are described by `q` as for p2r_run_queue; the arrays and the gradients are those of
+ * p2r_forward_backward (FP64 throughout, the stride-1 structure: every layer's propagated state
+ * is kept and the reverse starts each layer from it). Each warp keeps its slice's tape in its
+ * own region of the workspace and reuses it slice after slice, so the workspace is bounded by
+ * the resident warps, not by the batch: p2r_queue_adjoint_workspace_size(q) bytes (the slice
+ * and event partial sums, plus nlayer*27*32 doubles per resident warp on the current device); a
+ * smaller workspace runs fewer CTAs, at least one CTA's tapes is required. grad_dr_event /
+ * grad_bz_event: the same per event. Shared gradients are summed in a fixed order (per 32-lane
+ * slice, then per event, then in total): deterministic. Work items are checked on the device
+ * (p2r_queue_error reads the result from this workspace too). Flags other than 0 are
+ * rejected (P2R_ERR_UNSUPPORTED). nlayer <= 64, bsize a multiple of 32. */
+size_t p2r_queue_adjoint_workspace_size(const p2r_queue* q);
+int p2r_run_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hits, const float* dr, void* trk_out,
+                          float* chi2_out, const void* grad_trk_out, const float* grad_chi2, void* grad_trk_in,
+                          void* grad_hits, double* grad_dr, double* grad_bz, double* grad_dr_event,
+                          double* grad_bz_event, void* workspace, size_t workspace_bytes, void* stream);
+/* The same launch sequence (workspace clears, the persistent kernel, the fixed-order sums)
+ * captured once into a CUDA graph; replay with p2r_graph_launch. */
+int p2r_queue_adjoint_graph_create(const p2r_queue* q, const void* trk_in, const void* hits, const float* dr,
+                                   void* trk_out, float* chi2_out, const void* grad_trk_out, const float* grad_chi2,
+                                   void* grad_trk_in, void* grad_hits, double* grad_dr, double* grad_bz,
+                                   double* grad_dr_event, double* grad_bz_event, void* workspace,
+                                   size_t workspace_bytes, p2r_graph** out);
 
 /* ---------------------------------------------------------------- autotuning
  * Times p2r_forward on the caller's arrays for every (threads[i], stages[j]) pair

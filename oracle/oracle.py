@@ -6,6 +6,8 @@ the product package.
 
   Oracle      the project's own CPU restatement (p2r_oracle.cpp), float and double
   RefTBB      the reference's CPU path compiled unmodified (ref_harness.cpp -> _ref/)
+  RefGPU      the reference's own CUDA programs (cuda_v4.cu, cuda_uvm.cu) compiled
+              unmodified (ref_gpu_harness.cu -> _ref/), timed beside the product's kernel
   gen_helix   the benchmark's synthetic helix inputs (helix_gen.cpp), for the timed
               reference arm, which must map no library of the product
 """
@@ -110,6 +112,42 @@ def gen_helix(bsize: int, nevts: int, nb: int, nlayer: int, ntrk_event=None, nth
     return trk, hit
 
 
+def refgpu_available(kind: str) -> bool:
+    return (REF_DIR / f"libp2r_refgpu_{kind}.so").exists()
+
+
+class RefGPU:
+    """The reference's own CUDA programs compiled unmodified (ref_gpu_harness.cu -> _ref/):
+    kind 'v4' = GPUsequence (cuda_v4.cu:821-849, chained), 'uvm' = launch_p2r_kernel
+    (cuda_uvm.cu:887-915, restart). Sizes are compile-time (sizes())."""
+
+    def __init__(self, kind: str):
+        path = REF_DIR / f"libp2r_refgpu_{kind}.so"
+        if not path.exists():
+            raise RuntimeError(f"{path} missing: build it with `make -C oracle refgpu REFDIR=<reference checkout>`")
+        self.kind = kind
+        self.l = ctypes.CDLL(str(path))
+        self.l.refgpu_sizes.argtypes = [_vp, _vp, _vp, _vp]
+        self.l.refgpu_run.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]
+        self.l.refgpu_run.restype = ctypes.c_int
+        self.chained = bool(self.l.refgpu_chained())
+
+    def sizes(self):
+        """(nevts, nb, nlayer, bsize) the program was compiled for."""
+        ne, nb, nl, bs = ctypes.c_long(), ctypes.c_long(), ctypes.c_int(), ctypes.c_int()
+        self.l.refgpu_sizes(ctypes.byref(ne), ctypes.byref(nb), ctypes.byref(nl), ctypes.byref(bs))
+        return ne.value, nb.value, nl.value, bs.value
+
+    def run(self, trk_ptr: int, hit_ptr: int, out_ptr: int, warmup: int, iters: int, stream_ptr) -> float:
+        """Launches the kernel warmup + iters times on the stream (device pointers of arrays of
+        the compiled sizes); returns the CUDA-event milliseconds of the `iters` launches."""
+        ms = ctypes.c_float(0)
+        rc = self.l.refgpu_run(trk_ptr, hit_ptr, out_ptr, warmup, iters, stream_ptr, ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference GPU kernel ({self.kind}) failed: CUDA error {rc}")
+        return ms.value
+
+
 def host_isa() -> str:
     """'v4' when the host CPU has AVX-512 (F, BW, VL, DQ, CD), else 'v3'."""
     try:
@@ -151,10 +189,25 @@ class RefTBB:
         L.ref_get_kfact.restype = ctypes.c_float
         L.ref_propagate_block.argtypes = [_vp, _vp, _vp]
         L.ref_update_block.argtypes = [_vp, _vp]
+        L.ref_gain_inv_block.argtypes = [_vp, _vp, _vp]
+        L.ref_gain_block.argtypes = [_vp, _vp, _vp]
         L.ref_prepare_fixture.argtypes = [_vp, _vp]
         L.ref_fixture_raw.argtypes = [_vp, _vp, _vp, _vp]
         for n in ("ref_fixture_nevts", "ref_fixture_ntrks", "ref_fixture_nb"):
             getattr(L, n).restype = ctypes.c_long
+
+    def gain3(self, trk, hit, nblocks, nlayer, layer):
+        """The reference's unused KalmanGainInv / KalmanGain (TBB:376-426) per block, with the
+        hit of `layer`: returns (inv: nblocks x 9 x bsize, gain: nblocks x 18 x bsize)."""
+        bs = self.bsize
+        trk = np.ascontiguousarray(trk, np.float32).reshape(nblocks, 28 * bs)
+        hit = np.ascontiguousarray(hit, np.float32).reshape(nblocks * nlayer, 9 * bs)
+        inv = np.empty((nblocks, 9 * bs), np.float32)
+        gain = np.empty((nblocks, 18 * bs), np.float32)
+        for b in range(nblocks):
+            self.l.ref_gain_inv_block(trk[b].ctypes.data, hit[layer + b * nlayer].ctypes.data, inv[b].ctypes.data)
+            self.l.ref_gain_block(trk[b].ctypes.data, inv[b].ctypes.data, gain[b].ctypes.data)
+        return inv.reshape(nblocks, 9, bs), gain.reshape(nblocks, 18, bs)
 
     def set_bz(self, bz: float) -> None:
         if self.l.ref_set_bz(bz) != 0:

@@ -83,6 +83,19 @@ void ref_update_block(void* trk, const void* hit) {
   KalmanUpdate(&t->cov, &t->par, &h->cov, &h->pos);
 }
 
+// One Matriplex block: the reference's unused 3x3 routines (TBB:376-426). inv_out: an MP3x3
+// block (9*bsize floats); gain_out: an MP3x6 block (18*bsize floats).
+void ref_gain_inv_block(const void* trk, const void* hit, void* inv_out) {
+  const MPTRK* t = (const MPTRK*)trk;
+  const MPHIT* h = (const MPHIT*)hit;
+  KalmanGainInv(&t->cov, &h->cov, (MP3x3*)inv_out);
+}
+
+void ref_gain_block(const void* trk, const void* inv, void* gain_out) {
+  const MPTRK* t = (const MPTRK*)trk;
+  KalmanGain(&t->cov, (const MP3x3*)inv, (MP3x6*)gain_out);
+}
+
 // The reference driver loop (TBB:870-926) with run-time sizes. chained=0 is the
 // reference's "restart" form (every layer propagates the INPUT block, TBB:894);
 // chained=1 carries the output block from layer to layer, as the chained GPU

@@ -108,6 +108,8 @@ SIGNATURES = {
     "p2r_kfact": (ctypes.c_float, [ctypes.c_double]),
     "p2r_propagate_to_r": (ctypes.c_int, [_cfgp, _vp, _vp, _i32, _vp, _vp, _vp]),
     "p2r_kalman_update": (ctypes.c_int, [_cfgp, _vp, _vp, _i32, _vp, _vp]),
+    "p2r_kalman_gain_inv": (ctypes.c_int, [_cfgp, _vp, _vp, _i32, _vp, _vp]),
+    "p2r_kalman_gain": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp]),
     "p2r_forward": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "p2r_forward_masked": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "p2r_count_nonfinite": (ctypes.c_int, [_vp, _i64, _i32, _vp, _vp]),
@@ -125,6 +127,11 @@ SIGNATURES = {
     "p2r_autotune_forward": (ctypes.c_int, [_cfgp, _vp, _vp, _vp, _vp, _i32, _vp, _i32, _i32, _vp, _vp]),
     "p2r_queue_workspace_size": (ctypes.c_size_t, [_vp]),
     "p2r_queue_error": (ctypes.c_int, [_vp, _vp, _vp]),
+    "p2r_queue_adjoint_workspace_size": (ctypes.c_size_t, [_vp]),
+    "p2r_run_queue_adjoint": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                             _vp, ctypes.c_size_t, _vp]),
+    "p2r_queue_adjoint_graph_create": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                                      _vp, _vp, ctypes.c_size_t, _vp]),
     "p2r_run_queue": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "p2r_queue_graph_create": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp]),
     "p2r_graph_launch": (ctypes.c_int, [_vp, _vp]),

@@ -125,6 +125,26 @@ def KalmanUpdate(cfg: Config, trk, hits, layer: int, chi2_accum=None, stream=Non
                                   _arg(chi2_accum, "float32", cfg.ntracks, "chi2_accum"), _stream(stream)))
 
 
+def KalmanGainInv(cfg: Config, trk, hits, layer: int, inv_out, stream=None) -> None:
+    """The reference's unused KalmanGainInv (TBB:376-404) of every block with its hit in
+    `layer`: one MP3x3 block (9*bsize floats) per track block in inv_out."""
+    _check_shapes(cfg, trk, hits)
+    c = cfg.c()
+    check(lib().p2r_kalman_gain_inv(ctypes.byref(c), _ptr(trk), _ptr(hits), layer,
+                                    _arg(inv_out, "float32", cfg.nblocks * 9 * cfg.bsize, "inv_out"),
+                                    _stream(stream)))
+
+
+def KalmanGain(cfg: Config, trk, inv, gain_out, stream=None) -> None:
+    """The reference's unused KalmanGain (TBB:405-426): one MP3x6 block (18*bsize floats) per
+    track block in gain_out, from the track covariance and KalmanGainInv's output."""
+    _check_shapes(cfg, trk, None)
+    c = cfg.c()
+    check(lib().p2r_kalman_gain(ctypes.byref(c), _ptr(trk), _arg(inv, "float32", cfg.nblocks * 9 * cfg.bsize, "inv"),
+                                _arg(gain_out, "float32", cfg.nblocks * 18 * cfg.bsize, "gain_out"),
+                                _stream(stream)))
+
+
 def run_layers(cfg: Config, trk_in, hits, trk_out, stream=None) -> None:
     """The reference driver loop (TBB:878-923) issued layer by layer through the two calls."""
     trk_out.copy_(trk_in)

@@ -17,14 +17,17 @@
 // rounded to FP32 between layers still leaves 2e-3 on d chi2/d dr. P2R_FLAG_ADJ_FP32 selects
 // the FP32 kernel (the same code instantiated in float) where that accuracy suffices.
 //
-// Shared sums: each warp reduces with shuffles (fixed order) into per-warp partials in
+// Shared sums: each warp reduces with shuffles (fixed order) into per-warp double partials in
 // the workspace; a second kernel adds the partials in a fixed order in double, so the
 // results are deterministic run to run.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <new>
+
 #include "p2r_adjoint.cuh"
 #include "p2r_internal.h"
+#include "p2r_queue_check.cuh"
 
 namespace p2r {
 
@@ -42,7 +45,7 @@ struct AdjParams {
   const float* g_chi2;      // nullable, per-track cotangent of the summed chi2
   float* g_trk_in;          // nullable, Matriplex
   float* g_hits;            // nullable, Matriplex
-  float* partials;          // [nwarps][nlayer + 1]
+  double* partials;         // [nwarps][nlayer + 1]
   long long nblocks;
   int bsize;
   int nlayer;
@@ -76,7 +79,7 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
   const int it = (int)(g - b * bs);
   const bool valid = b < p.nblocks;
   const long long gwarp = g >> 5;
-  float* wpart = p.partials + gwarp * (p.nlayer + 1);
+  double* wpart = p.partials + gwarp * (p.nlayer + 1);
 
   T par[6] = {0, 0, 0, 1, 0, 1}, cov[21] = {};
   int q = 1;
@@ -188,12 +191,12 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
         for (int i = 0; i < 9; ++i) gh[i * bs + it] = 0.f;
       }
       drb = warp_sum_t(drb);
-      if (lane == 0) wpart[l] = (float)drb;
+      if (lane == 0) wpart[l] = (double)drb;
     }
   }
   // layers the whole warp skipped have zero gradient
   if (lane == 0)
-    for (int l = nl_warp; l < p.nlayer; ++l) wpart[l] = 0.f;
+    for (int l = nl_warp; l < p.nlayer; ++l) wpart[l] = 0.0;
   if (valid && p.g_hits)
     for (int l = nl_warp; l < p.nlayer; ++l) {
       float* gh = p.g_hits + (b * (long long)p.nlayer + l) * (9 * bs);
@@ -203,7 +206,7 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
   // k = q * kfact(Bz): dk/dBz = -k / Bz
   T bzb = valid ? (kbar - kinvbar * kinv * kinv) * (-k / (T)p.bz) : T(0);
   bzb = warp_sum_t(bzb);
-  if (lane == 0) wpart[p.nlayer] = (float)bzb;
+  if (lane == 0) wpart[p.nlayer] = (double)bzb;
   if (valid && p.g_trk_in) {
     float* gb = p.g_trk_in + b * (long long)(28 * bs);
 #pragma unroll
@@ -232,37 +235,42 @@ struct TapeParams {
   long long nthreads;
 };
 
+// One track's column of a tape: slot l, component i at base[l * slot + i * comp + idx].
 template <class T>
-__device__ __forceinline__ void tape_store(T* base, long long nthreads, long long g, const T (&par)[6],
-                                           const T (&cov)[21]) {
+struct TapeRef {
+  T* base;
+  long long slot, comp, idx;
+  __device__ __forceinline__ void store(long long l, const T (&par)[6], const T (&cov)[21]) const {
+    T* q = base + l * slot + idx;
 #pragma unroll
-  for (int i = 0; i < 6; ++i) base[i * nthreads + g] = par[i];
+    for (int i = 0; i < 6; ++i) q[i * comp] = par[i];
 #pragma unroll
-  for (int i = 0; i < 21; ++i) base[(6 + i) * nthreads + g] = cov[i];
-}
-template <class T>
-__device__ __forceinline__ void tape_load(const T* base, long long nthreads, long long g, T (&par)[6], T (&cov)[21]) {
+    for (int i = 0; i < 21; ++i) q[(6 + i) * comp] = cov[i];
+  }
+  __device__ __forceinline__ void load(long long l, T (&par)[6], T (&cov)[21]) const {
+    const T* q = base + l * slot + idx;
 #pragma unroll
-  for (int i = 0; i < 6; ++i) par[i] = base[i * nthreads + g];
+    for (int i = 0; i < 6; ++i) par[i] = q[i * comp];
 #pragma unroll
-  for (int i = 0; i < 21; ++i) cov[i] = base[(6 + i) * nthreads + g];
-}
+    for (int i = 0; i < 21; ++i) cov[i] = q[(6 + i) * comp];
+  }
+};
 
-// Per-thread set-up shared by both tape kernels.
+// Per-track set-up shared by the tape kernels and the queue kernel: track (block b, lane it)
+// of the Matriplex arrays, its initial state, layer count and k = q kfact.
 template <class T>
 struct TrackCtx {
-  long long g, b;
+  long long b;
   int it, lane, nl, nl_warp, q;
   bool valid;
   T k, kinv;
   const float* hblk;
-  __device__ TrackCtx(const AdjParams& p, T (&par)[6], T (&cov)[21]) {
+  __device__ TrackCtx(const AdjParams& p, T (&par)[6], T (&cov)[21], long long b_, int it_, bool valid_) {
     const int bs = p.bsize;
     lane = threadIdx.x & 31;
-    g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    b = g / bs;
-    it = (int)(g - b * bs);
-    valid = b < p.nblocks;
+    b = b_;
+    it = it_;
+    valid = valid_;
     q = 1;
     nl = 0;
 #pragma unroll
@@ -288,177 +296,103 @@ struct TrackCtx {
   }
 };
 
-template <class T, int CK>
-__global__ void __launch_bounds__(kAdjThreads) fwd_tape_kernel(AdjParams p, TapeParams tp) {
-  T par[6], cov[21];
-  const TrackCtx<T> c(p, par, cov);
+// The grid kernels' track: global thread g is lane it of block b.
+template <class T>
+__device__ __forceinline__ TrackCtx<T> grid_track(const AdjParams& p, T (&par)[6], T (&cov)[21], long long& g) {
+  g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long b = g / p.bsize;
+  return TrackCtx<T>(p, par, cov, b, (int)(g - b * p.bsize), b < p.nblocks);
+}
+
+template <class T>
+__device__ __forceinline__ void write_forward_outputs(const AdjParams& p, const TrackCtx<T>& c, const T (&par)[6],
+                                                      const T (&cov)[21], T chi2) {
+  if (!c.valid) return;
   const int bs = p.bsize;
-  T* tape = (T*)tp.tape;
+  if (p.trk_out) {
+    float* ob = p.trk_out + c.b * (long long)(28 * bs);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) ob[i * bs + c.it] = (float)par[i];
+#pragma unroll
+    for (int i = 0; i < 21; ++i) ob[(6 + i) * bs + c.it] = (float)cov[i];
+    ob[27 * bs + c.it] = __int_as_float(c.q);
+  }
+  if (p.chi2_out) p.chi2_out[c.b * bs + c.it] = (float)chi2;
+}
+
+// CK = 1 forward of one track: the state after each layer's propagation (entering its update)
+// goes to tape slot l; the final state and chi2 to the outputs.
+template <class T>
+__device__ __forceinline__ void fwd_track_ck1(const AdjParams& p, const TrackCtx<T>& c, T (&par)[6], T (&cov)[21],
+                                              const TapeRef<T>& tr) {
+  const int bs = p.bsize;
   T chi2 = 0;
   for (int l = 0; l < c.nl; ++l) {
     T hp[3], hc[6];
     load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
-    if constexpr (CK == 1) {
-      // the propagated state entering the update: the reverse starts each layer from it
-      adj::PropTape<T> t;
-      const T r = adj::hipo(hp[0], hp[1]) + (p.dr ? (T)p.dr[l] : T(0));
-      adj::prop_fwd(par, cov, c.k, c.kinv, r, t, par, cov);
-      tape_store(tape + (long long)l * 27 * tp.nthreads, tp.nthreads, c.g, par, cov);
-      chi2 += adj::upd_fwd(par, cov, hp, hc);
-    } else {
-      if (l % CK == 0) tape_store(tape + (long long)(l / CK) * 27 * tp.nthreads, tp.nthreads, c.g, par, cov);
-      chi2 += adj::layer_fwd(par, cov, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0));
-    }
+    adj::PropTape<T> t;
+    const T r = adj::hipo(hp[0], hp[1]) + (p.dr ? (T)p.dr[l] : T(0));
+    adj::prop_fwd(par, cov, c.k, c.kinv, r, t, par, cov);
+    tr.store(l, par, cov);
+    chi2 += adj::upd_fwd(par, cov, hp, hc);
   }
-  if (c.valid) {
-    if (p.trk_out) {
-      float* ob = p.trk_out + c.b * (long long)(28 * bs);
-#pragma unroll
-      for (int i = 0; i < 6; ++i) ob[i * bs + c.it] = (float)par[i];
-#pragma unroll
-      for (int i = 0; i < 21; ++i) ob[(6 + i) * bs + c.it] = (float)cov[i];
-      ob[27 * bs + c.it] = __int_as_float(c.q);
-    }
-    if (p.chi2_out) p.chi2_out[c.b * bs + c.it] = (float)chi2;
-  }
+  write_forward_outputs(p, c, par, cov, chi2);
 }
 
-template <class T, int CK>
-__global__ void __launch_bounds__(kAdjThreads) rev_tape_kernel(AdjParams p, TapeParams tp) {
-  T par[6], cov[21];
-  const TrackCtx<T> c(p, par, cov);
+// The cotangents of one track's final state and chi2.
+template <class T>
+__device__ __forceinline__ void load_seeds(const AdjParams& p, const TrackCtx<T>& c, T (&pb)[6], T (&cb)[21], T& chi2b) {
   const int bs = p.bsize;
-  const T* tape = (const T*)tp.tape;
-  T* segbuf = (T*)tp.segbuf;
-  float* wpart = p.partials + (c.g >> 5) * (p.nlayer + 1);
-  T pb[6] = {}, cb[21] = {};
-  T chi2b = 0;
-  if (c.valid) {
-    if (p.g_trk_out) {
-      const float* gb = p.g_trk_out + c.b * (long long)(28 * bs);
 #pragma unroll
-      for (int i = 0; i < 6; ++i) pb[i] = (T)gb[i * bs + c.it];
+  for (int i = 0; i < 6; ++i) pb[i] = 0;
 #pragma unroll
-      for (int i = 0; i < 21; ++i) cb[i] = (T)gb[(6 + i) * bs + c.it];
-    }
-    if (p.g_chi2) chi2b = (T)p.g_chi2[c.b * bs + c.it];
+  for (int i = 0; i < 21; ++i) cb[i] = 0;
+  chi2b = 0;
+  if (!c.valid) return;
+  if (p.g_trk_out) {
+    const float* gb = p.g_trk_out + c.b * (long long)(28 * bs);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) pb[i] = (T)gb[i * bs + c.it];
+#pragma unroll
+    for (int i = 0; i < 21; ++i) cb[i] = (T)gb[(6 + i) * bs + c.it];
   }
-  T kbar = 0, kinvbar = 0;
-  if constexpr (CK == 1) {
-    // Layer l, last to first: the update's reverse straight from the tape (the propagated state
-    // entering it), then the state entering the layer (the input track for l = 0, else the
-    // update of layer l-1 applied to its tape entry, as the forward did), the propagation's tape
-    // (its output covariance is not needed, so J C J^T is not recomputed) and its reverse.
-    for (int l = c.nl_warp - 1; l >= 0; --l) {
-      T drb = 0;
-      if (l < c.nl) {
-        T hp[3], hc[6], hpb[3], hcb[6];
-        load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
-        {
-          T up[6], uc[21];
-          tape_load(tape + (long long)l * 27 * tp.nthreads, tp.nthreads, c.g, up, uc);
-          adj::upd_rev(up, uc, hp, hc, pb, cb, chi2b, hpb, hcb);
-        }
-        T sp[6], sc[21];
-        if (l == 0) {
-          const float* tb = p.trk_in + c.b * (long long)(28 * bs);
+  if (p.g_chi2) chi2b = (T)p.g_chi2[c.b * bs + c.it];
+}
+
+template <class T>
+__device__ __forceinline__ void write_hit_grads(const AdjParams& p, const TrackCtx<T>& c, int l, const T (&hpb)[3],
+                                                const T (&hcb)[6]) {
+  if (!p.g_hits) return;
+  const int bs = p.bsize;
+  float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
 #pragma unroll
-          for (int i = 0; i < 6; ++i) sp[i] = (T)tb[i * bs + c.it];
+  for (int i = 0; i < 3; ++i) gh[i * bs + c.it] = (float)hpb[i];
 #pragma unroll
-          for (int i = 0; i < 21; ++i) sc[i] = (T)tb[(6 + i) * bs + c.it];
-        } else {
-          T hq[3], hqc[6];
-          tape_load(tape + (long long)(l - 1) * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
-          load_hit_t(c.hblk + (long long)(l - 1) * (9 * bs), bs, c.it, hq, hqc);
-          adj::upd_fwd(sp, sc, hq, hqc);
-        }
-        const T rh = adj::hipo(hp[0], hp[1]);
-        const T r = rh + (p.dr ? (T)p.dr[l] : T(0));
-        adj::PropTape<T> t;
-        T pp[6], pc[21];
-        adj::prop_fwd(sp, sc, c.k, c.kinv, r, t, pp, pc);
-        T pin[6], cin[21], rbar = 0;
-        adj::prop_rev(t, sp, sc, c.k, c.kinv, r, pb, cb, pin, cin, rbar, kbar, kinvbar);
+  for (int i = 0; i < 6; ++i) gh[(3 + i) * bs + c.it] = (float)hcb[i];
+}
+
+template <class T>
+__device__ __forceinline__ void zero_hit_grads(const AdjParams& p, const TrackCtx<T>& c, int l) {
+  if (!c.valid || !p.g_hits) return;
+  const int bs = p.bsize;
+  float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
 #pragma unroll
-        for (int i = 0; i < 6; ++i) pb[i] = pin[i];
-#pragma unroll
-        for (int i = 0; i < 21; ++i) cb[i] = cin[i];
-        drb = rbar;
-        if (rh > T(0)) {
-          const T irh = T(1) / rh;
-          hpb[0] += rbar * hp[0] * irh;
-          hpb[1] += rbar * hp[1] * irh;
-        }
-        if (p.g_hits) {
-          float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
-#pragma unroll
-          for (int i = 0; i < 3; ++i) gh[i * bs + c.it] = (float)hpb[i];
-#pragma unroll
-          for (int i = 0; i < 6; ++i) gh[(3 + i) * bs + c.it] = (float)hcb[i];
-        }
-      } else if (c.valid && p.g_hits) {
-        float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) gh[i * bs + c.it] = 0.f;
-      }
-      drb = warp_sum_t(drb);
-      if (c.lane == 0) wpart[l] = (float)drb;
-    }
-  }
-  const int nseg = CK == 1 ? 0 : (c.nl_warp + CK - 1) / CK;
-  for (int seg = nseg - 1; seg >= 0; --seg) {
-    const int a = seg * CK;
-    const int e = min(a + CK, c.nl_warp);
-    if (CK > 1 && a + 1 < min(e, c.nl)) {
-      // states before layers a+1 .. e-1, recomputed once from the checkpoint
-      T sp[6], sc[21];
-      tape_load(tape + (long long)seg * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
-      for (int l = a + 1; l < e && l < c.nl; ++l) {
-        T hp[3], hc[6];
-        load_hit_t(c.hblk + (long long)(l - 1) * (9 * bs), bs, c.it, hp, hc);
-        adj::layer_fwd(sp, sc, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l - 1] : T(0));
-        tape_store(segbuf + (long long)(l - a - 1) * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
-      }
-    }
-    for (int l = e - 1; l >= a; --l) {
-      T drb = 0;
-      if (l < c.nl) {
-        T sp[6], sc[21];
-        if (l == a)
-          tape_load(tape + (long long)seg * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
-        else
-          tape_load(segbuf + (long long)(l - a - 1) * 27 * tp.nthreads, tp.nthreads, c.g, sp, sc);
-        T hp[3], hc[6], hpb[3], hcb[6];
-        load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
-        adj::layer_rev(sp, sc, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0), pb, cb, chi2b, hpb, hcb, drb, kbar,
-                       kinvbar);
-        if (p.g_hits) {
-          float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
-#pragma unroll
-          for (int i = 0; i < 3; ++i) gh[i * bs + c.it] = (float)hpb[i];
-#pragma unroll
-          for (int i = 0; i < 6; ++i) gh[(3 + i) * bs + c.it] = (float)hcb[i];
-        }
-      } else if (c.valid && p.g_hits) {
-        float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
-#pragma unroll
-        for (int i = 0; i < 9; ++i) gh[i * bs + c.it] = 0.f;
-      }
-      drb = warp_sum_t(drb);
-      if (c.lane == 0) wpart[l] = (float)drb;
-    }
-  }
+  for (int i = 0; i < 9; ++i) gh[i * bs + c.it] = 0.f;
+}
+
+// End of one track's reverse sweep: zero gradients of layers the whole warp skipped, the warp's
+// Bz partial (lane 0 writes wpart[nlayer]) and the initial-state gradient.
+template <class T>
+__device__ __forceinline__ void finish_track(const AdjParams& p, const TrackCtx<T>& c, const T (&pb)[6],
+                                             const T (&cb)[21], T kbar, T kinvbar, double* wpart) {
+  const int bs = p.bsize;
   if (c.lane == 0)
-    for (int l = c.nl_warp; l < p.nlayer; ++l) wpart[l] = 0.f;
-  if (c.valid && p.g_hits)
-    for (int l = c.nl_warp; l < p.nlayer; ++l) {
-      float* gh = p.g_hits + (c.b * (long long)p.nlayer + l) * (9 * bs);
-#pragma unroll
-      for (int i = 0; i < 9; ++i) gh[i * bs + c.it] = 0.f;
-    }
+    for (int l = c.nl_warp; l < p.nlayer; ++l) wpart[l] = 0.0;
+  for (int l = c.nl_warp; l < p.nlayer; ++l) zero_hit_grads(p, c, l);
+  // k = q * kfact(Bz): dk/dBz = -k / Bz
   T bzb = c.valid ? (kbar - kinvbar * c.kinv * c.kinv) * (-c.k / (T)p.bz) : T(0);
   bzb = warp_sum_t(bzb);
-  if (c.lane == 0) wpart[p.nlayer] = (float)bzb;
+  if (c.lane == 0) wpart[p.nlayer] = (double)bzb;
   if (c.valid && p.g_trk_in) {
     float* gb = p.g_trk_in + c.b * (long long)(28 * bs);
 #pragma unroll
@@ -469,16 +403,207 @@ __global__ void __launch_bounds__(kAdjThreads) rev_tape_kernel(AdjParams p, Tape
   }
 }
 
+// CK = 1 reverse of one track from its tape. Layer l, last to first: the update's reverse
+// straight from the tape (the propagated state entering it), then the state entering the layer
+// (the input track for l = 0, else the update of layer l-1 applied to its tape entry, as the
+// forward did), the propagation's tape (its output covariance is not needed, so J C J^T is not
+// recomputed) and its reverse. Lane 0 writes the warp's dr and Bz partials to wpart.
+template <class T>
+__device__ __forceinline__ void rev_track_ck1(const AdjParams& p, const TrackCtx<T>& c, const TapeRef<T>& tr,
+                                              double* wpart) {
+  const int bs = p.bsize;
+  T pb[6], cb[21], chi2b;
+  load_seeds(p, c, pb, cb, chi2b);
+  T kbar = 0, kinvbar = 0;
+  for (int l = c.nl_warp - 1; l >= 0; --l) {
+    T drb = 0;
+    if (l < c.nl) {
+      T hp[3], hc[6], hpb[3], hcb[6];
+      load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
+      {
+        T up[6], uc[21];
+        tr.load(l, up, uc);
+        adj::upd_rev(up, uc, hp, hc, pb, cb, chi2b, hpb, hcb);
+      }
+      T sp[6], sc[21];
+      if (l == 0) {
+        const float* tb = p.trk_in + c.b * (long long)(28 * bs);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) sp[i] = (T)tb[i * bs + c.it];
+#pragma unroll
+        for (int i = 0; i < 21; ++i) sc[i] = (T)tb[(6 + i) * bs + c.it];
+      } else {
+        T hq[3], hqc[6];
+        tr.load(l - 1, sp, sc);
+        load_hit_t(c.hblk + (long long)(l - 1) * (9 * bs), bs, c.it, hq, hqc);
+        adj::upd_fwd(sp, sc, hq, hqc);
+      }
+      const T rh = adj::hipo(hp[0], hp[1]);
+      const T r = rh + (p.dr ? (T)p.dr[l] : T(0));
+      adj::PropTape<T> t;
+      T pp[6], pc[21];
+      adj::prop_fwd(sp, sc, c.k, c.kinv, r, t, pp, pc);
+      T pin[6], cin[21], rbar = 0;
+      adj::prop_rev(t, sp, sc, c.k, c.kinv, r, pb, cb, pin, cin, rbar, kbar, kinvbar);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) pb[i] = pin[i];
+#pragma unroll
+      for (int i = 0; i < 21; ++i) cb[i] = cin[i];
+      drb = rbar;
+      if (rh > T(0)) {
+        const T irh = T(1) / rh;
+        hpb[0] += rbar * hp[0] * irh;
+        hpb[1] += rbar * hp[1] * irh;
+      }
+      write_hit_grads(p, c, l, hpb, hcb);
+    } else {
+      zero_hit_grads(p, c, l);
+    }
+    drb = warp_sum_t(drb);
+    if (c.lane == 0) wpart[l] = (double)drb;
+  }
+  finish_track(p, c, pb, cb, kbar, kinvbar, wpart);
+}
+
+template <class T, int CK>
+__global__ void __launch_bounds__(kAdjThreads) fwd_tape_kernel(AdjParams p, TapeParams tp) {
+  T par[6], cov[21];
+  long long g;
+  const TrackCtx<T> c = grid_track(p, par, cov, g);
+  const int bs = p.bsize;
+  const TapeRef<T> tr{(T*)tp.tape, 27 * tp.nthreads, tp.nthreads, g};
+  if constexpr (CK == 1) {
+    fwd_track_ck1(p, c, par, cov, tr);
+  } else {
+    T chi2 = 0;
+    for (int l = 0; l < c.nl; ++l) {
+      T hp[3], hc[6];
+      load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
+      if (l % CK == 0) tr.store(l / CK, par, cov);
+      chi2 += adj::layer_fwd(par, cov, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0));
+    }
+    write_forward_outputs(p, c, par, cov, chi2);
+  }
+}
+
+template <class T, int CK>
+__global__ void __launch_bounds__(kAdjThreads) rev_tape_kernel(AdjParams p, TapeParams tp) {
+  T par[6], cov[21];
+  long long g;
+  const TrackCtx<T> c = grid_track(p, par, cov, g);
+  const int bs = p.bsize;
+  const TapeRef<T> tr{(T*)tp.tape, 27 * tp.nthreads, tp.nthreads, g};
+  double* wpart = p.partials + (g >> 5) * (p.nlayer + 1);
+  if constexpr (CK == 1) {
+    rev_track_ck1(p, c, tr, wpart);
+  } else {
+    const TapeRef<T> sr{(T*)tp.segbuf, 27 * tp.nthreads, tp.nthreads, g};
+    T pb[6], cb[21], chi2b;
+    load_seeds(p, c, pb, cb, chi2b);
+    T kbar = 0, kinvbar = 0;
+    const int nseg = (c.nl_warp + CK - 1) / CK;
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+      const int a = seg * CK;
+      const int e = min(a + CK, c.nl_warp);
+      if (a + 1 < min(e, c.nl)) {
+        // states before layers a+1 .. e-1, recomputed once from the checkpoint
+        T sp[6], sc[21];
+        tr.load(seg, sp, sc);
+        for (int l = a + 1; l < e && l < c.nl; ++l) {
+          T hp[3], hc[6];
+          load_hit_t(c.hblk + (long long)(l - 1) * (9 * bs), bs, c.it, hp, hc);
+          adj::layer_fwd(sp, sc, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l - 1] : T(0));
+          sr.store(l - a - 1, sp, sc);
+        }
+      }
+      for (int l = e - 1; l >= a; --l) {
+        T drb = 0;
+        if (l < c.nl) {
+          T sp[6], sc[21];
+          if (l == a)
+            tr.load(seg, sp, sc);
+          else
+            sr.load(l - a - 1, sp, sc);
+          T hp[3], hc[6], hpb[3], hcb[6];
+          load_hit_t(c.hblk + (long long)l * (9 * bs), bs, c.it, hp, hc);
+          adj::layer_rev(sp, sc, c.k, c.kinv, hp, hc, p.dr ? (T)p.dr[l] : T(0), pb, cb, chi2b, hpb, hcb, drb, kbar,
+                         kinvbar);
+          write_hit_grads(p, c, l, hpb, hcb);
+        } else {
+          zero_hit_grads(p, c, l);
+        }
+        drb = warp_sum_t(drb);
+        if (c.lane == 0) wpart[l] = (double)drb;
+      }
+    }
+    finish_track(p, c, pb, cb, kbar, kinvbar, wpart);
+  }
+}
+
+// ---------------------------------------------------------------- persistent queue path
+// Forward + adjoint of an uneven batch in ONE persistent launch: CTAs pull (event, block range)
+// items from the queue's atomic counter (the items are checked on the device first, as in the
+// forward queue kernel); each warp takes 32-lane slices of an item's blocks and runs, per lane,
+// the CK = 1 forward (FP64, propagated states to the warp's own tape) and then the reverse from
+// that tape. A warp's tape is [nlayer][27][32] doubles in the workspace, reused slice after
+// slice, so the memory is bounded by the resident warps (not by the batch) and the reverse reads
+// back the most recently written entries first, while they are still in L2. Shared-gradient
+// partials go to a per-slice row (slice = block * (bsize / 32) + 32-lane group), summed per event
+// and then in total in a fixed order: deterministic, and the same per-slice order as the
+// per-warp partials of the grid kernels.
+struct QAdjParams {
+  const p2r_queue_item* items;
+  long long n_items;
+  const int64_t* ev_off;
+  long long nevts;
+  int* counter;
+  unsigned* error;
+  double* tapes;          // [tape_warps][nlayer][27][32]
+  double* slice_partials; // [nblocks * bsize / 32][nlayer + 1]
+};
+
+__global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAdjParams q) {
+  __shared__ long long s_item;
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int spb = p.bsize / 32;
+  const long long tstride = (long long)p.nlayer * 27 * 32;
+  double* tape = q.tapes + ((long long)blockIdx.x * nwarps + warp) * tstride;
+  const TapeRef<double> tr{tape, 27 * 32, 32, lane};
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(q.counter, 1);
+    __syncthreads();
+    const long long item = s_item;
+    __syncthreads();  // every thread has read s_item before thread 0 claims the next one
+    if (item >= q.n_items) break;
+    const p2r_queue_item qi = q.items[item];
+    const unsigned bad = queue_item_error(qi, q.nevts, p.nblocks, q.ev_off);
+    if (bad) {
+      if (threadIdx.x == 0) atomicOr(q.error, bad);
+      continue;
+    }
+    const int nslices = qi.nblk * spb;
+    for (int s = warp; s < nslices; s += nwarps) {
+      const long long b = qi.block0 + s / spb;
+      const int it = (s % spb) * 32 + lane;
+      double par[6], cov[21];
+      const TrackCtx<double> c(p, par, cov, b, it, true);
+      fwd_track_ck1(p, c, par, cov, tr);
+      rev_track_ck1(p, c, tr, q.slice_partials + (b * spb + s % spb) * (p.nlayer + 1));
+    }
+  }
+}
+
 // Sums per-warp partials [nwarps][nout] in a fixed order, in double. Block (e, j) sums
 // warps [e*wpe, min((e+1)*wpe, nwarps)) of column j into out[e*nout + j].
-__global__ void __launch_bounds__(256) sum_partials_kernel(const float* partials, long long nwarps, int nout,
+__global__ void __launch_bounds__(256) sum_partials_kernel(const double* partials, long long nwarps, int nout,
                                                            long long wpe, double* out) {
   __shared__ double red[256];
   const long long e = blockIdx.x;
   const int j = blockIdx.y;
   const long long w0 = e * wpe, w1 = min(w0 + wpe, nwarps);
   double s = 0.0;
-  for (long long w = w0 + threadIdx.x; w < w1; w += blockDim.x) s += (double)partials[w * nout + j];
+  for (long long w = w0 + threadIdx.x; w < w1; w += blockDim.x) s += partials[w * nout + j];
   red[threadIdx.x] = s;
   __syncthreads();
   for (int o = 128; o > 0; o >>= 1) {
@@ -515,7 +640,7 @@ using namespace p2r;
 
 namespace {
 
-// workspace: float partials[nwarps][nlayer+1], then (8-byte aligned) double
+// workspace: double partials[nwarps][nlayer+1], then (256-byte aligned) double
 // event_sums[nevts][nlayer+1] and double totals[nlayer+1]
 struct WsLayout {
   long long nwarps;
@@ -527,7 +652,7 @@ WsLayout layout_of(const p2r_config* cfg) {
   const long long ntr = (long long)cfg->nevts * cfg->nb * cfg->bsize;
   const long long nthreads = (ntr + kAdjThreads - 1) / kAdjThreads * kAdjThreads;
   w.nwarps = nthreads / 32;
-  w.partial_bytes = (size_t)w.nwarps * (cfg->nlayer + 1) * sizeof(float);
+  w.partial_bytes = (size_t)w.nwarps * (cfg->nlayer + 1) * sizeof(double);
   w.event_off = (w.partial_bytes + 255) & ~(size_t)255;
   w.total_off = w.event_off + (((size_t)cfg->nevts * (cfg->nlayer + 1) * sizeof(double) + 255) & ~(size_t)255);
   w.total_bytes = w.total_off + (size_t)(cfg->nlayer + 1) * sizeof(double);
@@ -671,7 +796,7 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   p.g_chi2 = grad_chi2;
   p.g_trk_in = (float*)grad_trk_in;
   p.g_hits = (float*)grad_hits;
-  p.partials = (float*)workspace;
+  p.partials = (double*)workspace;
   p.nblocks = nblocks;
   p.bsize = cfg->bsize;
   p.nlayer = cfg->nlayer;
@@ -836,3 +961,248 @@ extern "C" int p2r_forward_backward_noalloc(const p2r_config* cfg, const void* t
                               grad_trk_in, grad_hits, grad_dr, grad_bz, grad_dr_event, grad_bz_event, ckpt_stride,
                               ws, kNoAllocScratchBytes, stream);
 }
+
+// ---------------------------------------------------------------- persistent queue entry points
+namespace p2r {
+
+// Per-event sums of the per-slice partials: block (e, j) adds slices [b0 * spb, b1 * spb) of
+// column j, [b0, b1) = event e's block range (clamped to [0, nblocks]; bad offsets are reported
+// by the queue checks), in the same fixed order as sum_partials_kernel.
+__global__ void __launch_bounds__(256) sum_slices_kernel(const double* partials, const int64_t* ev_off,
+                                                         long long nblocks, int spb, int nout, double* out) {
+  __shared__ double red[256];
+  const long long e = blockIdx.x;
+  const int j = blockIdx.y;
+  long long b0 = ev_off[e], b1 = ev_off[e + 1];
+  b0 = b0 < 0 ? 0 : (b0 > nblocks ? nblocks : b0);
+  b1 = b1 < b0 ? b0 : (b1 > nblocks ? nblocks : b1);
+  const long long w0 = b0 * spb, w1 = b1 * spb;
+  double s = 0.0;
+  for (long long w = w0 + threadIdx.x; w < w1; w += blockDim.x) s += partials[w * nout + j];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[e * nout + j] = red[0];
+}
+
+}  // namespace p2r
+
+namespace {
+
+// Queue-adjoint workspace: item counter (0) and error word (128) as every queue workspace, then
+// double slice partials [nslices][nlayer+1], event sums [nevts][nlayer+1], totals [nlayer+1],
+// then the warps' tapes [tape_warps][nlayer][27][32] doubles.
+struct QAdjWs {
+  long long nslices;
+  size_t partial_off, event_off, total_off, tape_off, per_warp_tape;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+QAdjWs qadj_ws(const p2r_queue* q) {
+  QAdjWs w;
+  const size_t nout = (size_t)q->nlayer + 1;
+  w.nslices = q->nblocks * (q->bsize / 32);
+  w.partial_off = 256;
+  w.event_off = align256(w.partial_off + (size_t)w.nslices * nout * sizeof(double));
+  w.total_off = align256(w.event_off + (size_t)q->nevts * nout * sizeof(double));
+  w.tape_off = align256(w.total_off + nout * sizeof(double));
+  w.per_warp_tape = (size_t)q->nlayer * 27 * 32 * sizeof(double);
+  return w;
+}
+
+// Resident CTAs of the queue-adjoint kernel on the current device (the persistent grid).
+int qadj_resident_ctas(const p2r_queue* q, int threads, int* out) {
+  int dev = 0, sms = 0, occ = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, queue_adj_kernel, threads, 0);
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "queue adjoint: %s", cudaGetErrorString(e));
+  const int per_sm = q->ctas_per_sm > 0 ? (q->ctas_per_sm < occ ? q->ctas_per_sm : occ) : occ;
+  *out = sms * (per_sm > 0 ? per_sm : 1);
+  return P2R_OK;
+}
+
+int qadj_threads(const p2r_queue* q) { return q->block_threads > 0 ? q->block_threads : kAdjThreads; }
+
+int check_queue_adjoint(const p2r_queue* q, const char* who) {
+  int rc = p2r_check_queue(q, who);
+  if (rc) return rc;
+  if (q->flags & (P2R_FLAG_SQUASH_PHI | P2R_FLAG_ADJ_FP32 | P2R_FLAG_FP32_DET))
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: the queue adjoint runs in FP64 without option flags", who);
+  if (q->nlayer > kMaxAdjLayers)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: nlayer %d exceeds %d", who, q->nlayer, kMaxAdjLayers);
+  return P2R_OK;
+}
+
+int enqueue_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hits, const float* dr, void* trk_out,
+                          float* chi2_out, const void* grad_trk_out, const float* grad_chi2, void* grad_trk_in,
+                          void* grad_hits, double* grad_dr, double* grad_bz, double* grad_dr_event,
+                          double* grad_bz_event, void* workspace, size_t ws_bytes, cudaStream_t st, const char* who) {
+  P2rRange range(who);
+  int rc = check_queue_adjoint(q, who);
+  if (rc) return rc;
+  const QAdjWs w = qadj_ws(q);
+  const int threads = qadj_threads(q);
+  const int wpc = threads / 32;
+  if (!workspace || ws_bytes < w.tape_off + w.per_warp_tape * wpc)
+    return p2r_set_errorf(P2R_ERR_WORKSPACE, "%s: workspace of at least %zu bytes needed (%zu for full occupancy: "
+                          "p2r_queue_adjoint_workspace_size)", who, w.tape_off + w.per_warp_tape * wpc,
+                          p2r_queue_adjoint_workspace_size(q));
+  if (((uintptr_t)workspace & 255u) != 0) return p2r_set_errorf(P2R_ERR_INVALID, "%s: workspace must be 256-byte aligned", who);
+  if (q->nevts == 0) return p2r_clear_error();
+  if (!trk_in || !hits) return p2r_set_errorf(P2R_ERR_INVALID, "%s: null input array", who);
+  if ((rc = p2r_check_aligned(who, 4, {trk_in, hits, dr, q->nlay_lane, trk_out, chi2_out, grad_trk_out, grad_chi2,
+                                       grad_trk_in, grad_hits})) ||
+      (rc = p2r_check_aligned(who, 8, {grad_dr, grad_bz, grad_dr_event, grad_bz_event, q->event_block_offset,
+                                       q->items})))
+    return rc;
+  {
+    const size_t tb = (size_t)q->nblocks * 28 * q->bsize * sizeof(float);
+    const size_t hb = (size_t)q->nblocks * q->nlayer * 9 * q->bsize * sizeof(float);
+    const size_t lb = (size_t)q->nblocks * q->bsize * sizeof(float);
+    const size_t nl = (size_t)q->nlayer, ne = (size_t)q->nevts;
+    if ((rc = p2r_check_spans(
+             who, {{"trk_in", trk_in, tb, false},
+                   {"hits", hits, hb, false},
+                   {"dr", dr, nl * sizeof(float), false},
+                   {"nlay_lane", q->nlay_lane, lb, false},
+                   {"event_block_offset", q->event_block_offset, (ne + 1) * sizeof(int64_t), false},
+                   {"items", q->items, (size_t)q->n_items * sizeof(p2r_queue_item), false},
+                   {"grad_trk_out", grad_trk_out, tb, false},
+                   {"grad_chi2", grad_chi2, lb, false},
+                   {"trk_out", trk_out, tb, true},
+                   {"chi2_out", chi2_out, lb, true},
+                   {"grad_trk_in", grad_trk_in, tb, true},
+                   {"grad_hits", grad_hits, hb, true},
+                   {"grad_dr", grad_dr, nl * sizeof(double), true},
+                   {"grad_bz", grad_bz, sizeof(double), true},
+                   {"grad_dr_event", grad_dr_event, ne * nl * sizeof(double), true},
+                   {"grad_bz_event", grad_bz_event, ne * sizeof(double), true},
+                   {"workspace", workspace, ws_bytes, true}})))
+      return rc;
+  }
+  int resident = 0;
+  if ((rc = qadj_resident_ctas(q, threads, &resident))) return rc;
+  const long long tape_ctas = (long long)((ws_bytes - w.tape_off) / (w.per_warp_tape * wpc));
+  long long grid = resident < tape_ctas ? resident : tape_ctas;
+  if (grid > q->n_items) grid = q->n_items;
+  if (grid < 1) grid = 1;
+  AdjParams p;
+  p.trk_in = (const float*)trk_in;
+  p.hits = (const float*)hits;
+  p.dr = dr;
+  p.nlay = q->nlay_lane;
+  p.trk_out = (float*)trk_out;
+  p.chi2_out = chi2_out;
+  p.g_trk_out = (const float*)grad_trk_out;
+  p.g_chi2 = grad_chi2;
+  p.g_trk_in = (float*)grad_trk_in;
+  p.g_hits = (float*)grad_hits;
+  p.partials = nullptr;
+  p.nblocks = q->nblocks;
+  p.bsize = q->bsize;
+  p.nlayer = q->nlayer;
+  p.kfact = p2r_kfact_of(q->bz);
+  p.bz = q->bz == 0.0 ? 3.8112 : q->bz;
+  QAdjParams qp;
+  qp.items = q->items;
+  qp.n_items = q->n_items;
+  qp.ev_off = q->event_block_offset;
+  qp.nevts = q->nevts;
+  qp.counter = (int*)((char*)workspace + kQueueCounterOff);
+  qp.error = (unsigned*)((char*)workspace + kQueueErrorOff);
+  qp.slice_partials = (double*)((char*)workspace + w.partial_off);
+  qp.tapes = (double*)((char*)workspace + w.tape_off);
+  // counter and error word cleared; slice partials zeroed (slices of skipped items add nothing)
+  cudaError_t e = cudaMemsetAsync(workspace, 0, 256, st);
+  if (e == cudaSuccess && w.nslices > 0)
+    e = cudaMemsetAsync(qp.slice_partials, 0, (size_t)w.nslices * (q->nlayer + 1) * sizeof(double), st);
+  if (e == cudaSuccess && q->n_items > 0) {
+    queue_adj_kernel<<<(unsigned)grid, threads, 0, st>>>(p, qp);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: launch failed: %s", who, cudaGetErrorString(e));
+  const int nout = q->nlayer + 1;
+  double* ev = (double*)((char*)workspace + w.event_off);
+  double* tot = (double*)((char*)workspace + w.total_off);
+  sum_slices_kernel<<<dim3((unsigned)q->nevts, (unsigned)nout), 256, 0, st>>>(
+      qp.slice_partials, q->event_block_offset, q->nblocks, q->bsize / 32, nout, ev);
+  sum_rows_kernel<<<(nout + 63) / 64, 64, 0, st>>>(ev, q->nevts, nout, tot);
+  if (grad_dr || grad_bz) split_kernel<<<(nout + 63) / 64, 64, 0, st>>>(tot, 1, q->nlayer, grad_dr, grad_bz);
+  if (grad_dr_event || grad_bz_event)
+    split_kernel<<<(unsigned)((q->nevts * nout + 255) / 256), 256, 0, st>>>(ev, q->nevts, q->nlayer, grad_dr_event,
+                                                                            grad_bz_event);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: reduction launch failed: %s", who, cudaGetErrorString(e));
+  return p2r_clear_error();
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t p2r_queue_adjoint_workspace_size(const p2r_queue* q) {
+  const char* who = "p2r_queue_adjoint_workspace_size";
+  if (check_queue_adjoint(q, who)) return 0;
+  const QAdjWs w = qadj_ws(q);
+  const int threads = qadj_threads(q);
+  int resident = 0;
+  if (qadj_resident_ctas(q, threads, &resident)) return 0;
+  long long ctas = resident < q->n_items ? resident : q->n_items;
+  if (ctas < 1) ctas = 1;
+  p2r_clear_error();
+  return w.tape_off + (size_t)ctas * (threads / 32) * w.per_warp_tape;
+}
+
+int p2r_run_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hits, const float* dr, void* trk_out,
+                          float* chi2_out, const void* grad_trk_out, const float* grad_chi2, void* grad_trk_in,
+                          void* grad_hits, double* grad_dr, double* grad_bz, double* grad_dr_event,
+                          double* grad_bz_event, void* workspace, size_t workspace_bytes, void* stream) {
+  return enqueue_queue_adjoint(q, trk_in, hits, dr, trk_out, chi2_out, grad_trk_out, grad_chi2, grad_trk_in,
+                               grad_hits, grad_dr, grad_bz, grad_dr_event, grad_bz_event, workspace, workspace_bytes,
+                               (cudaStream_t)stream, "p2r_run_queue_adjoint");
+}
+
+int p2r_queue_adjoint_graph_create(const p2r_queue* q, const void* trk_in, const void* hits, const float* dr,
+                                   void* trk_out, float* chi2_out, const void* grad_trk_out, const float* grad_chi2,
+                                   void* grad_trk_in, void* grad_hits, double* grad_dr, double* grad_bz,
+                                   double* grad_dr_event, double* grad_bz_event, void* workspace,
+                                   size_t workspace_bytes, p2r_graph** out) {
+  const char* who = "p2r_queue_adjoint_graph_create";
+  if (!out) return p2r_set_errorf(P2R_ERR_INVALID, "%s: out is null", who);
+  *out = nullptr;
+  int rc = check_queue_adjoint(q, who);
+  if (rc) return rc;
+  cudaStream_t cs;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
+  p2r_graph* g = new (std::nothrow) p2r_graph();
+  if (!g) {
+    cudaStreamDestroy(cs);
+    return p2r_set_errorf(P2R_ERR_INVALID, "%s: out of host memory", who);
+  }
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = enqueue_queue_adjoint(q, trk_in, hits, dr, trk_out, chi2_out, grad_trk_out, grad_chi2, grad_trk_in,
+                               grad_hits, grad_dr, grad_bz, grad_dr_event, grad_bz_event, workspace, workspace_bytes,
+                               cs, who);
+    cudaError_t e2 = cudaStreamEndCapture(cs, &g->graph);
+    if (!rc && e2 != cudaSuccess) e = e2;
+  }
+  if (!rc && e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  cudaStreamDestroy(cs);
+  if (rc || e != cudaSuccess) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return rc ? rc : p2r_set_errorf(P2R_ERR_CUDA, "%s: %s", who, cudaGetErrorString(e));
+  }
+  *out = g;
+  return p2r_clear_error();
+}
+
+}  // extern "C"

@@ -27,6 +27,15 @@
 #define P2R_UNROLL
 #endif
 
+// Precision-study markers: each names the arithmetic region the statements after it belong to
+// (path, covprop, upd in the forward functions; pathrev, covrev, jbar, jent, updrec, updrev in
+// the reverse ones). They expand to nothing unless a study build defines P2R_PREC_REGION
+// (tests/precision_study/adjoint_precision.cpp, which runs this code with chosen regions
+// rounded to FP32).
+#ifndef P2R_PREC_REGION
+#define P2R_PREC_REGION(name)
+#endif
+
 namespace p2r {
 namespace adj {
 
@@ -83,6 +92,7 @@ struct PropTape {
 template <class T>
 P2R_HD void prop_fwd(const T (&ip)[6], const T (&ic)[21], T k, T kinv, T r, PropTape<T>& t, T (&op)[6],
                      T (&oc)[21]) {
+  P2R_PREC_REGION(path);
   const T xin = ip[0], yin = ip[1], zin = ip[2], iptin = ip[3], phiin = ip[4], thetain = ip[5];
   t.r00 = hipo(xin, yin);
   t.pt = T(1) / iptin;
@@ -167,6 +177,7 @@ P2R_UNROLL
   t.J41 = dady;
   t.J43 = dadipt;
   t.J44 = T(1) + dadphi;
+  P2R_PREC_REGION(covprop);
   // rows 0, 1, 2, 4 of J*C (rows 3 and 5 are rows 3 and 5 of C); not kept on the tape:
   // the reverse forms J-bar as (S J) C instead of S (J C)
   T T0[6], T1[6], T2[6], T4[6];
@@ -197,6 +208,7 @@ P2R_UNROLL
     if (i >= 3) oc[S6(i, 3)] = Ti[3];
     if (i >= 5) oc[S6(i, 5)] = Ti[5];
   }
+  P2R_PREC_REGION(path);
   op[0] = xo;
   op[1] = yo;
   op[2] = zin + k * alpha * cT * pt * isT;
@@ -212,6 +224,7 @@ template <class T>
 P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], T k, T kinv, T r,
                      const T (&pb_out)[6], const T (&cb_out)[21], T (&pb_in)[6], T (&cb_in)[21], T& rbar, T& kbar,
                      T& kinvbar) {
+  P2R_PREC_REGION(pathrev);
   const T x = ip[0], y = ip[1], ipt = ip[3];
   const T pt = t.pt, cP = t.cP, sP = t.sP, ca = t.ca, sa = t.sa, cT = t.cT, sT = t.sT, isT = t.isT;
   const T alpha = t.alpha, dadx = t.dadx, dady = t.dady, dadipt = t.dadipt, dadphi = t.dadphi;
@@ -226,6 +239,7 @@ P2R_HD void prop_rev(const PropTape<T>& t, const T (&ip)[6], const T (&ic)[21], 
   T ptb = zb * k * alpha * cT * isT;
   T isTb = zb * k * alpha * cT * pt;
 
+  P2R_PREC_REGION(covrev);
   // ---- C' = J C J^T: S = Gbar + Gbar^T, Jbar = S (J C) = (S J) C, cbar = packed(J^T S J)
   T S[6][6];
 P2R_UNROLL
@@ -256,6 +270,7 @@ P2R_UNROLL
     for (int i = j; i < 6; ++i) cb_in[S6(i, j)] = i == j ? T(0.5f) * M[i] : M[i];
   }
 
+  P2R_PREC_REGION(jbar);
   // Jbar = W C at the non-trivial entries of J
   auto WC = [&](int a, int b) {
     T s = 0;
@@ -268,6 +283,7 @@ P2R_UNROLL
   const T J20b = WC(2, 0), J21b = WC(2, 1), J23b = WC(2, 3), J24b = WC(2, 4), J25b = WC(2, 5);
   const T J40b = WC(4, 0), J41b = WC(4, 1), J43b = WC(4, 3), J44b = WC(4, 4);
 
+  P2R_PREC_REGION(jent);
   // ---- Jacobian entries -> their inputs
   const T U = cP * ca - sP * sa, V = sP * ca + cP * sa, w = ipt * dadipt;
   T Ub = 0, Vb = 0, wb = 0, dadxb = 0, dadyb = 0, dadiptb = 0, dadphib = 0, cPb = 0, sPb = 0;
@@ -339,6 +355,7 @@ P2R_UNROLL
   alphab += sincos4_bar(alpha, sab, cab);
   thetab += -cTb * sT - isTb * cT * isT * isT;
 
+  P2R_PREC_REGION(pathrev);
   // ---- alpha, dad* from D and the path derivatives
   T Db = alphab * ipt * kinv + dadiptb * kinv;
   iptb += alphab * t.D * kinv + dadxb * t.dDdx * kinv + dadyb * t.dDdy * kinv + dadiptb * t.dDdipt * kinv +
@@ -470,6 +487,7 @@ P2R_UNROLL
 // determinant is taken in double (TBB:457).
 template <class T>
 P2R_HD T upd_fwd(T (&p)[6], T (&c)[21], const T (&hp)[3], const T (&hc)[6]) {
+  P2R_PREC_REGION(upd);
   const T rh = hipo(hp[0], hp[1]);
   const T ih = T(0.5f) / rh;
   const T R00 = -(hp[1] + p[1]) * ih;
@@ -506,6 +524,7 @@ P2R_UNROLL
 template <class T>
 P2R_HD void upd_rev(const T (&p)[6], const T (&c)[21], const T (&hp)[3], const T (&hc)[6], T (&pb)[6], T (&cb)[21],
                     T chi2b, T (&hpb)[3], T (&hcb)[6]) {
+  P2R_PREC_REGION(updrec);
   const T rh = hipo(hp[0], hp[1]);
   const T den = T(2) * rh;
   const T iden = T(1) / den;  // one reciprocal for every quotient by den (and by rh = den / 2)
@@ -527,6 +546,7 @@ P2R_UNROLL
   }
   const T res0 = R00 * (hp[0] - p[0]) + R01 * (hp[1] - p[1]), res1 = hp[2] - p[2];
 
+  P2R_PREC_REGION(updrev);
   // C' = C - K0 B0^T - K1 B1^T (lower triangle); p' = p + K0 res0 + K1 res1
   T K0b[6], K1b[6], B0b[6], B1b[6];
 P2R_UNROLL

@@ -5,6 +5,7 @@
 
 #include <initializer_list>
 
+#include <cuda_runtime_api.h>
 #include <nvtx3/nvToolsExt.h>
 
 #include "../../include/p2r.h"
@@ -52,6 +53,16 @@ struct P2rRange {
   ~P2rRange() { nvtxRangePop(); }
   P2rRange(const P2rRange&) = delete;
   P2rRange& operator=(const P2rRange&) = delete;
+};
+
+// Validates a p2r_queue description's sizes and options on the host (not its device arrays,
+// which the kernels check); returns P2R_OK or an error status with a message.
+int p2r_check_queue(const p2r_queue* q, const char* who);
+
+// A captured launch sequence (p2r_queue_graph_create, p2r_queue_adjoint_graph_create).
+struct p2r_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
 };
 
 // kfact exactly as the reference rounds it (TBB:654); bz == 0 means 3.8112 T.

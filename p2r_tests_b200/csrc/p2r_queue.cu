@@ -19,6 +19,7 @@
 
 #include "p2r_fwd.cuh"
 #include "p2r_internal.h"
+#include "p2r_queue_check.cuh"
 
 namespace p2r {
 
@@ -40,12 +41,6 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-
-// Error bits of the queue's device-side checks (the word p2r_queue_error reads).
-constexpr unsigned kQerrEvent = 1u;       // an item's event outside [0, nevts)
-constexpr unsigned kQerrBlocks = 2u;      // an item's blocks outside [0, nblocks) or nblk < 0
-constexpr unsigned kQerrEventRange = 4u;  // an item's blocks outside its event's block range
-constexpr unsigned kQerrOffsets = 8u;     // event offsets decreasing, outside [0, nblocks], or too large
 
 __global__ void queue_init_kernel(const int64_t* ev_off, long long nevts, long long nblocks, int slices_per_block,
                                   int* counter, int* ev_remaining, unsigned* error, unsigned long long* t_start) {
@@ -84,14 +79,7 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
     const p2r_queue_item qi = q.items[item];
     // the items are device data the host did not re-read: an item outside the arrays is
     // skipped and reported (p2r_queue_error), never indexed
-    unsigned bad = 0u;
-    if (qi.event < 0 || qi.event >= q.nevts) {
-      bad = kQerrEvent;
-    } else if (qi.nblk < 0 || qi.block0 < 0 || qi.block0 > q.f.nblocks - qi.nblk) {
-      bad = kQerrBlocks;
-    } else if (qi.block0 < q.ev_off[qi.event] || qi.block0 + qi.nblk > q.ev_off[qi.event + 1]) {
-      bad = kQerrEventRange;
-    }
+    const unsigned bad = queue_item_error(qi, q.nevts, q.f.nblocks, q.ev_off);
     if (bad) {
       if (threadIdx.x == 0) atomicOr(q.error, bad);
       continue;
@@ -147,15 +135,17 @@ struct QueueWs {
 
 QueueWs queue_ws(int64_t nevts) {
   QueueWs w;
-  w.counter_off = 0;
-  w.error_off = 128;
+  w.counter_off = kQueueCounterOff;
+  w.error_off = kQueueErrorOff;
   w.start_off = 256;
   w.remaining_off = 512;
   w.bytes = 512 + (((size_t)nevts * sizeof(int) + 255) & ~(size_t)255);
   return w;
 }
 
-int check_queue(const p2r_queue* q, const char* who) {
+}  // namespace
+
+int p2r_check_queue(const p2r_queue* q, const char* who) {
   if (!q) return p2r_set_errorf(P2R_ERR_INVALID, "%s: queue is null", who);
   if (q->bsize < 32 || q->bsize % 32 != 0 || q->bsize > 4096)
     return p2r_set_errorf(P2R_ERR_QUEUE, "%s: bsize %d must be a multiple of 32", who, q->bsize);
@@ -175,11 +165,13 @@ int check_queue(const p2r_queue* q, const char* who) {
   return P2R_OK;
 }
 
+namespace {
+
 int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void* trk_out, float* chi2_out,
                   unsigned long long* event_done_ns, unsigned long long* start_ns, void* workspace, size_t ws_bytes,
                   cudaStream_t st, const char* who) {
   P2rRange range(who);
-  int rc = check_queue(q, who);
+  int rc = p2r_check_queue(q, who);
   if (rc) return rc;
   const QueueWs w = queue_ws(q->nevts);
   if (!workspace || ws_bytes < w.bytes)
@@ -267,11 +259,6 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
 
 }  // namespace
 
-struct p2r_graph {
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-};
-
 extern "C" {
 
 int64_t p2r_queue_plan(const int64_t* host_event_block_offset, int64_t nevts, int32_t blocks_per_item,
@@ -332,7 +319,7 @@ int p2r_queue_graph_create(const p2r_queue* q, const void* trk_in, const void* h
                            size_t ws_bytes, p2r_graph** out) {
   if (!out) return p2r_set_error(P2R_ERR_INVALID, "p2r_queue_graph_create: out is null");
   *out = nullptr;
-  int rc = check_queue(q, "p2r_queue_graph_create");
+  int rc = p2r_check_queue(q, "p2r_queue_graph_create");
   if (rc) return rc;
   cudaStream_t cs;
   cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
