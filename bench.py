@@ -738,6 +738,35 @@ def main():
         bms_sorted = b0.elapsed_time(b1) / args.calib_steps
         dr_rel = float(((out4s["grad_dr"] - out4["grad_dr"]).abs().max() / out4["grad_dr"].abs().max()).item())
         del out4s, t4s, h4s, nl4s
+        # the same forward + adjoint in ONE persistent launch over the work queue (per-warp tapes,
+        # the workspace bounded by the resident warps), captured in a CUDA graph; plain and with
+        # each event's tracks ordered by layer count inside the launch
+        wq = {"event_block_offset": np.arange(c4.nevts + 1, dtype=np.int64) * c4.nb,
+              "nlay_lane": nl4.cpu().numpy(), "nblocks": c4.nblocks, "bsize": c4.bsize, "nlayer": c4.nlayer,
+              "bz": c4.bz}
+        qadj = {}
+        for name, fl in (("plain", 0), ("ordered_by_layers", p2r.FLAG_ORDER_BY_LAYERS)):
+            qa = p2r.Queue(wq, blocks_per_item=4, flags=fl)
+            oq = qa.capture_adjoint(t4, h4, dr=dr4, grad_chi2=gc4, out={"grad_trk_in": None, "grad_hits": None})
+            qa.replay(stream)
+            torch.cuda.synchronize()
+            b0.record(stream)
+            for _ in range(args.calib_steps):
+                qa.replay(stream)
+            b1.record(stream)
+            torch.cuda.synchronize()
+            qms = b0.elapsed_time(b1) / args.calib_steps
+            ref_ev, ref_bz = out4["grad_dr_event"], out4["grad_bz_event"]
+            qadj[name] = {
+                "ms_per_step": qms, "ratio_vs_forward": qms / fms, "updates_per_s": upd4 / (qms / 1e3),
+                "workspace_bytes": int(oq["workspace"].numel()), "queue_errors": qa.error_bits(stream),
+                "grad_dr_event_max_rel_diff_vs_grid_path": float(
+                    ((oq["grad_dr_event"] - ref_ev).abs().max() / ref_ev.abs().max()).item()),
+                "grad_bz_event_max_rel_diff_vs_grid_path": float(
+                    ((oq["grad_bz_event"] - ref_bz).abs().max() / ref_bz.abs().max()).item())}
+            qa.release()
+            del oq, qa
+        del wq
         calib = {"workload": f"{c4.ntracks // c4.nevts} tracks x {c4.nevts} events x 40 layers, hits on r = 4..110 cm, "
                              "20-40 layers per track (uniform), dr ~ U[-100, 100] um, generated on the device",
                  "hits_bytes": h4.numel() * 4, "tracks_bytes": t4.numel() * 4, "updates": upd4,
@@ -746,7 +775,15 @@ def main():
                              "api": "p2r_forward_masked (fused, per-track layer counts)",
                              "sorted_by_layer_count": {"ms_per_step": fms_sorted,
                                                        "updates_per_s": upd4 / (fms_sorted / 1e3)}},
-                 "forward_adjoint": {"ms_per_step": bms, "ratio_vs_forward": bms / fms, "ckpt_stride": ck4,
+                 "forward_adjoint": {
+                     "ms_per_step": qadj["ordered_by_layers"]["ms_per_step"],
+                     "ratio_vs_forward": qadj["ordered_by_layers"]["ratio_vs_forward"],
+                     "ratio_vs_forward_sorted": qadj["ordered_by_layers"]["ms_per_step"] / fms_sorted,
+                     "api": "p2r_queue_adjoint_graph_create (P2R_FLAG_ORDER_BY_LAYERS): one CUDA graph of the "
+                            "workspace clears, the per-event ordering by layer count, ONE persistent FP64 "
+                            "forward + adjoint launch over the work queue, and the fixed-order per-event sums",
+                     "persistent_queue": qadj},
+                 "forward_adjoint_grid_path": {"ms_per_step": bms, "ratio_vs_forward": bms / fms, "ckpt_stride": ck4,
                                      "workspace_bytes": p2r.workspace_size(c4, ck4),
                                      "sorted_by_layer_count": {
                                          "ms_per_step": bms_sorted,

@@ -62,6 +62,11 @@ typedef enum p2r_mode { P2R_MODE_RESTART = 0, P2R_MODE_CHAINED = 1 } p2r_mode;
 #define P2R_FLAG_SQUASH_PHI 0x8u /* wrap phi into [-pi, pi] after every update: the step the reference
                                     leaves commented out (squashPhiMPlex, TBB:635); forward entry points,
                                     with the FP64 determinant (not with P2R_FLAG_FP32_DET) */
+#define P2R_FLAG_ORDER_BY_LAYERS 0x10u /* p2r_queue.flags of the queue adjoint: inside the launch, order
+                                    each event's tracks by layer count (longest first, ties in track
+                                    order) so a warp's lanes run tracks of similar length; outputs stay
+                                    at each track's own position, per-track results are the same
+                                    arithmetic, the shared sums are added in the new grouping */
 
 typedef struct p2r_config {
   int32_t bsize;         /* Matriplex lanes per block (TBB:15-17); >= 1 */
@@ -205,7 +210,8 @@ size_t p2r_queue_workspace_size(const p2r_queue* q);
 /* After a p2r_run_queue (or graph launch) on `stream` with this workspace: synchronises the
  * stream and returns P2R_ERR_QUEUE if the device skipped malformed work items or event offsets
  * (host_bits receives the reasons: 1 event outside [0, nevts), 2 blocks outside [0, nblocks),
- * 4 blocks outside the item's event range, 8 event offsets decreasing or outside [0, nblocks]),
+ * 4 blocks outside the item's event range, 8 event offsets decreasing or outside [0, nblocks],
+ * 16 a queue-adjoint track-order entry outside the batch),
  * P2R_OK otherwise. */
 int p2r_queue_error(const void* workspace, uint32_t* host_bits, void* stream);
 
@@ -268,7 +274,7 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
  * captures a CUDA graph, event loops that forbid allocation after start-up, plugin hosts whose
  * device memory belongs to the host framework's pool. Batches whose workspace
  * (p2r_forward_backward_workspace_size) exceeds 8 MiB are rejected with P2R_ERR_WORKSPACE
- * (about 3 M tracks at 20 layers, fewer with more layers or events). The array has its own
+ * (about 1.5 M tracks at 20 layers, fewer with more layers or events). The array has its own
  * address in every CUDA context (each device's primary context, and any context a plugin
  * host creates and makes current): the first call in each context looks that address up
  * (cudaGetSymbolAddress, with the context current) and caches it under the context's unique
@@ -292,7 +298,9 @@ int p2r_forward_backward_noalloc(const p2r_config* cfg, const void* trk_in, cons
  * smaller workspace runs fewer CTAs, at least one CTA's tapes is required. grad_dr_event /
  * grad_bz_event: the same per event. Shared gradients are summed in a fixed order (per 32-lane
  * slice, then per event, then in total): deterministic. Work items are checked on the device
- * (p2r_queue_error reads the result from this workspace too). Flags other than 0 are
+ * (p2r_queue_error reads the result from this workspace too; bit 16: a track-order entry outside
+ * the batch, which overlapping event ranges can cause). q->flags: 0 or P2R_FLAG_ORDER_BY_LAYERS
+ * (the ordering runs inside the launch: one stable counting sort per event); other flags are
  * rejected (P2R_ERR_UNSUPPORTED). nlayer <= 64, bsize a multiple of 32. */
 size_t p2r_queue_adjoint_workspace_size(const p2r_queue* q);
 int p2r_run_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hits, const float* dr, void* trk_out,

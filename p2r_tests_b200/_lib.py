@@ -27,6 +27,7 @@ FLAG_FP32_DET = 0x1
 FLAG_NO_STAGING = 0x2
 FLAG_ADJ_FP32 = 0x4
 FLAG_SQUASH_PHI = 0x8
+FLAG_ORDER_BY_LAYERS = 0x10
 MATH_REFINED, MATH_IEEE, MATH_FAST = 0, 1, 2
 
 

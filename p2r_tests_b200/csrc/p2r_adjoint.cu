@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <climits>
 #include <new>
 
 #include "p2r_adjoint.cuh"
@@ -560,6 +561,7 @@ struct QAdjParams {
   unsigned* error;
   double* tapes;          // [tape_warps][nlayer][27][32]
   double* slice_partials; // [nblocks * bsize / 32][nlayer + 1]
+  const uint32_t* order;  // nullable: track at each position, each event's tracks by layer count
 };
 
 __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAdjParams q) {
@@ -583,14 +585,86 @@ __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAd
       continue;
     }
     const int nslices = qi.nblk * spb;
+    const long long ntr = p.nblocks * p.bsize;
     for (int s = warp; s < nslices; s += nwarps) {
-      const long long b = qi.block0 + s / spb;
-      const int it = (s % spb) * 32 + lane;
+      // position (block b, lane it) of the batch; with an order, the track placed there
+      long long b = qi.block0 + s / spb;
+      int it = (s % spb) * 32 + lane;
+      const long long slice = b * spb + s % spb;
+      bool valid = true;
+      if (q.order) {
+        const long long t = q.order[b * p.bsize + it];
+        valid = t < ntr;  // written by the ordering kernel for every position of a valid item
+        if (!valid) atomicOr(q.error, kQerrOrder);
+        b = valid ? t / p.bsize : 0;
+        it = valid ? (int)(t - b * p.bsize) : 0;
+      }
       double par[6], cov[21];
-      const TrackCtx<double> c(p, par, cov, b, it, true);
+      const TrackCtx<double> c(p, par, cov, b, it, valid);
       fwd_track_ck1(p, c, par, cov, tr);
-      rev_track_ck1(p, c, tr, q.slice_partials + (b * spb + s % spb) * (p.nlayer + 1));
+      rev_track_ck1(p, c, tr, q.slice_partials + slice * (p.nlayer + 1));
     }
+  }
+}
+
+// Each event's tracks ordered by layer count, longest first, ties in track order (a stable
+// counting sort; one CTA per event): order[pos] = the track placed at position pos of the
+// event's range. Keys nlayer - clamp(nlay, 0, nlayer) ascending; per chunk of 512 tracks each
+// lane's rank among equal keys comes from its warp (__match_any_sync) and the warps before it.
+constexpr int kOrderThreads = 512;
+__global__ void __launch_bounds__(kOrderThreads) order_by_layers_kernel(const int32_t* nlay, const int64_t* ev_off,
+                                                                       long long nblocks, int bsize, int nlayer,
+                                                                       uint32_t* order) {
+  constexpr int kW = kOrderThreads / 32;
+  __shared__ int hist[kMaxAdjLayers + 1];
+  __shared__ long long base[kMaxAdjLayers + 1];
+  __shared__ int wcount[kW][kMaxAdjLayers + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nkeys = nlayer + 1;
+  const long long e = blockIdx.x;
+  long long b0 = ev_off[e], b1 = ev_off[e + 1];
+  b0 = b0 < 0 ? 0 : (b0 > nblocks ? nblocks : b0);
+  b1 = b1 < b0 ? b0 : (b1 > nblocks ? nblocks : b1);
+  const long long t0 = b0 * bsize, t1 = b1 * bsize;
+  auto key = [&](long long t) {
+    const int v = nlay[t];
+    return nlayer - (v < 0 ? 0 : (v > nlayer ? nlayer : v));
+  };
+  for (int k = tid; k < nkeys; k += kOrderThreads) hist[k] = 0;
+  __syncthreads();
+  for (long long t = t0 + tid; t < t1; t += kOrderThreads) atomicAdd(&hist[key(t)], 1);
+  __syncthreads();
+  if (tid == 0) {
+    long long run = t0;
+    for (int k = 0; k < nkeys; ++k) {
+      base[k] = run;
+      run += hist[k];
+    }
+  }
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+  for (long long c = t0; c < t1; c += kOrderThreads) {
+    const long long t = c + tid;
+    const bool valid = t < t1;
+    const int k = valid ? key(t) : -1;
+    const unsigned same = __match_any_sync(0xffffffffu, k);
+    const int rank = __popc(same & lt);
+    for (int j = lane; j < nkeys; j += 32) wcount[warp][j] = 0;
+    __syncwarp();
+    if (valid && rank == 0) wcount[warp][k] = __popc(same);
+    __syncthreads();
+    if (valid) {
+      long long pre = base[k] + rank;
+      for (int w = 0; w < warp; ++w) pre += wcount[w][k];
+      order[pre] = (uint32_t)t;
+    }
+    __syncthreads();
+    for (int j = tid; j < nkeys; j += kOrderThreads) {
+      long long add = 0;
+      for (int w = 0; w < kW; ++w) add += wcount[w][j];
+      base[j] += add;
+    }
+    __syncthreads();
   }
 }
 
@@ -948,7 +1022,7 @@ extern "C" int p2r_forward_backward_noalloc(const p2r_config* cfg, const void* t
   if (need > kNoAllocScratchBytes)
     return p2r_set_errorf(P2R_ERR_WORKSPACE,
                           "p2r_forward_backward_noalloc: this batch needs %zu bytes of scratch; the allocation-free "
-                          "entry point has a fixed %zu bytes per GPU (about (tracks/32)*(nlayer+1)*4 + "
+                          "entry point has a fixed %zu bytes per GPU (about (tracks/32)*(nlayer+1)*8 + "
                           "nevts*(nlayer+1)*8 bytes are used): split the batch or pass a workspace to "
                           "p2r_forward_backward",
                           need, kNoAllocScratchBytes);
@@ -994,10 +1068,11 @@ namespace {
 
 // Queue-adjoint workspace: item counter (0) and error word (128) as every queue workspace, then
 // double slice partials [nslices][nlayer+1], event sums [nevts][nlayer+1], totals [nlayer+1],
-// then the warps' tapes [tape_warps][nlayer][27][32] doubles.
+// with P2R_FLAG_ORDER_BY_LAYERS the track order [nblocks * bsize] (uint32), then the warps'
+// tapes [tape_warps][nlayer][27][32] doubles.
 struct QAdjWs {
   long long nslices;
-  size_t partial_off, event_off, total_off, tape_off, per_warp_tape;
+  size_t partial_off, event_off, total_off, order_off, tape_off, per_warp_tape;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -1009,7 +1084,9 @@ QAdjWs qadj_ws(const p2r_queue* q) {
   w.partial_off = 256;
   w.event_off = align256(w.partial_off + (size_t)w.nslices * nout * sizeof(double));
   w.total_off = align256(w.event_off + (size_t)q->nevts * nout * sizeof(double));
-  w.tape_off = align256(w.total_off + nout * sizeof(double));
+  w.order_off = align256(w.total_off + nout * sizeof(double));
+  const bool ordered = (q->flags & P2R_FLAG_ORDER_BY_LAYERS) != 0;
+  w.tape_off = align256(w.order_off + (ordered ? (size_t)q->nblocks * q->bsize * sizeof(uint32_t) : 0));
   w.per_warp_tape = (size_t)q->nlayer * 27 * 32 * sizeof(double);
   return w;
 }
@@ -1031,8 +1108,11 @@ int qadj_threads(const p2r_queue* q) { return q->block_threads > 0 ? q->block_th
 int check_queue_adjoint(const p2r_queue* q, const char* who) {
   int rc = p2r_check_queue(q, who);
   if (rc) return rc;
-  if (q->flags & (P2R_FLAG_SQUASH_PHI | P2R_FLAG_ADJ_FP32 | P2R_FLAG_FP32_DET))
-    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: the queue adjoint runs in FP64 without option flags", who);
+  if (q->flags & ~(uint32_t)P2R_FLAG_ORDER_BY_LAYERS)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED,
+                          "%s: the queue adjoint runs in FP64; P2R_FLAG_ORDER_BY_LAYERS is its only option", who);
+  if ((q->flags & P2R_FLAG_ORDER_BY_LAYERS) && q->nblocks * (long long)q->bsize > (long long)UINT32_MAX)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: ordering needs fewer than 2^32 tracks", who);
   if (q->nlayer > kMaxAdjLayers)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: nlayer %d exceeds %d", who, q->nlayer, kMaxAdjLayers);
   return P2R_OK;
@@ -1117,10 +1197,16 @@ int enqueue_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hi
   qp.error = (unsigned*)((char*)workspace + kQueueErrorOff);
   qp.slice_partials = (double*)((char*)workspace + w.partial_off);
   qp.tapes = (double*)((char*)workspace + w.tape_off);
+  qp.order = (q->flags & P2R_FLAG_ORDER_BY_LAYERS) ? (const uint32_t*)((char*)workspace + w.order_off) : nullptr;
   // counter and error word cleared; slice partials zeroed (slices of skipped items add nothing)
   cudaError_t e = cudaMemsetAsync(workspace, 0, 256, st);
   if (e == cudaSuccess && w.nslices > 0)
     e = cudaMemsetAsync(qp.slice_partials, 0, (size_t)w.nslices * (q->nlayer + 1) * sizeof(double), st);
+  if (e == cudaSuccess && qp.order && q->nblocks > 0) {
+    order_by_layers_kernel<<<(unsigned)q->nevts, kOrderThreads, 0, st>>>(
+        q->nlay_lane, q->event_block_offset, q->nblocks, q->bsize, q->nlayer, (uint32_t*)qp.order);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess && q->n_items > 0) {
     queue_adj_kernel<<<(unsigned)grid, threads, 0, st>>>(p, qp);
     e = cudaGetLastError();

@@ -173,6 +173,8 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
   P2rRange range(who);
   int rc = p2r_check_queue(q, who);
   if (rc) return rc;
+  if (q->flags & P2R_FLAG_ORDER_BY_LAYERS)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_ORDER_BY_LAYERS is an option of the queue adjoint", who);
   const QueueWs w = queue_ws(q->nevts);
   if (!workspace || ws_bytes < w.bytes)
     return p2r_set_errorf(P2R_ERR_WORKSPACE, "%s: workspace of %zu bytes needed", who, w.bytes);

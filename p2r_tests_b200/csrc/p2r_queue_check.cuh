@@ -15,6 +15,7 @@ constexpr unsigned kQerrEvent = 1u;       // an item's event outside [0, nevts)
 constexpr unsigned kQerrBlocks = 2u;      // an item's blocks outside [0, nblocks) or nblk < 0
 constexpr unsigned kQerrEventRange = 4u;  // an item's blocks outside its event's block range
 constexpr unsigned kQerrOffsets = 8u;     // event offsets decreasing, outside [0, nblocks], or too large
+constexpr unsigned kQerrOrder = 16u;      // a track order entry outside the batch (offsets that overlap)
 
 // Byte offsets in every queue workspace: the item counter and the error word.
 constexpr size_t kQueueCounterOff = 0;

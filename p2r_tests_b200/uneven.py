@@ -173,6 +173,7 @@ class Queue:
                 _arg(trk_out, "float32", ntrk * TRK_WORDS, "trk_out"), _arg(chi2, "float32", ntrk, "chi2"))
 
     def run(self, trk_in, hits, trk_out, chi2=None, stream=None) -> None:
+        self._last_ws = self.ws
         check(lib().p2r_run_queue(ctypes.byref(self.q), *self._arrays(trk_in, hits, trk_out, chi2),
                                   _ptr(self.done_ns), _ptr(self.start_ns), _ptr(self.ws), self.ws.numel(),
                                   _stream(stream)))
@@ -180,6 +181,7 @@ class Queue:
     def capture(self, trk_in, hits, trk_out, chi2=None) -> None:
         """Captures the launch sequence into a CUDA graph (pointers are baked in)."""
         self.release()
+        self._last_ws = self.ws
         g = ctypes.c_void_p()
         check(lib().p2r_queue_graph_create(ctypes.byref(self.q), *self._arrays(trk_in, hits, trk_out, chi2),
                                            _ptr(self.done_ns), _ptr(self.start_ns), _ptr(self.ws), self.ws.numel(),
@@ -196,11 +198,74 @@ class Queue:
             lib().p2r_graph_destroy(self.graph)
             self.graph = None
 
+    # ------------------------------------------------------------ forward + adjoint
+    def adjoint_workspace_size(self) -> int:
+        n = lib().p2r_queue_adjoint_workspace_size(ctypes.byref(self.q))
+        if n == 0:
+            raise P2RError(_lib.P2R_ERR_INVALID, lib().p2r_last_error_string().decode())
+        return int(n)
+
+    def _adjoint_args(self, trk_in, hits, dr, grad_trk_out, grad_chi2, o: dict):
+        """The argument list of p2r_run_queue_adjoint / p2r_queue_adjoint_graph_create after
+        the queue, each array checked for type and size against the workload."""
+        torch = self.torch
+        w = self.w
+        ntrk = w["nblocks"] * w["bsize"]
+        nt, nh, nl = ntrk * TRK_WORDS, ntrk * w["nlayer"] * HIT_WORDS, w["nlayer"]
+        dev = trk_in.device
+        f32 = dict(dtype=torch.float32, device=dev)
+        f64 = dict(dtype=torch.float64, device=dev)
+        o.setdefault("trk_out", torch.empty_like(trk_in))
+        o.setdefault("chi2", torch.empty(ntrk, **f32))
+        o.setdefault("grad_trk_in", torch.empty_like(trk_in))
+        o.setdefault("grad_hits", torch.empty_like(hits))
+        o.setdefault("grad_dr", torch.empty(nl, **f64))
+        o.setdefault("grad_bz", torch.empty(1, **f64))
+        o.setdefault("grad_dr_event", torch.empty(self.nevts, nl, **f64))
+        o.setdefault("grad_bz_event", torch.empty(self.nevts, **f64))
+        need = self.adjoint_workspace_size()
+        ws = o.get("workspace")
+        if ws is None or ws.numel() < need:
+            ws = torch.empty(need, dtype=torch.uint8, device=dev)
+            o["workspace"] = ws
+        return (_arg(trk_in, "float32", nt, "trk_in"), _arg(hits, "float32", nh, "hits"),
+                _arg(dr, "float32", nl, "dr"), _arg(o["trk_out"], "float32", nt, "trk_out"),
+                _arg(o["chi2"], "float32", ntrk, "chi2"), _arg(grad_trk_out, "float32", nt, "grad_trk_out"),
+                _arg(grad_chi2, "float32", ntrk, "grad_chi2"), _arg(o["grad_trk_in"], "float32", nt, "grad_trk_in"),
+                _arg(o["grad_hits"], "float32", nh, "grad_hits"), _arg(o["grad_dr"], "float64", nl, "grad_dr"),
+                _arg(o["grad_bz"], "float64", 1, "grad_bz"),
+                _arg(o["grad_dr_event"], "float64", self.nevts * nl, "grad_dr_event"),
+                _arg(o["grad_bz_event"], "float64", self.nevts, "grad_bz_event"), _ptr(ws), ws.numel())
+
+    def run_adjoint(self, trk_in, hits, dr=None, grad_trk_out=None, grad_chi2=None, out=None, stream=None) -> dict:
+        """Forward + adjoint of the batch in one persistent launch (p2r_run_queue_adjoint):
+        returns trk_out, chi2, grad_trk_in, grad_hits, grad_dr, grad_bz, grad_dr_event,
+        grad_bz_event (an entry of `out` set to None skips that output) and the workspace."""
+        o = out if out is not None else {}
+        args = self._adjoint_args(trk_in, hits, dr, grad_trk_out, grad_chi2, o)
+        self._last_ws = o["workspace"]
+        check(lib().p2r_run_queue_adjoint(ctypes.byref(self.q), *args, _stream(stream)))
+        return o
+
+    def capture_adjoint(self, trk_in, hits, dr=None, grad_trk_out=None, grad_chi2=None, out=None) -> dict:
+        """Captures the forward + adjoint launch sequence into a CUDA graph (replay()); returns
+        the output dict the replays write."""
+        self.release()
+        o = out if out is not None else {}
+        args = self._adjoint_args(trk_in, hits, dr, grad_trk_out, grad_chi2, o)
+        self._last_ws = o["workspace"]
+        g = ctypes.c_void_p()
+        check(lib().p2r_queue_adjoint_graph_create(ctypes.byref(self.q), *args, ctypes.byref(g)))
+        self.graph = g
+        self.adjoint_out = o
+        return o
+
     def error_bits(self, stream=None) -> int:
         """Synchronises `stream` and returns the device-side check bits of the last launch
         (0: every work item and event offset was in range; see p2r_queue_error)."""
         bits = ctypes.c_uint32(0)
-        rc = lib().p2r_queue_error(_ptr(self.ws), ctypes.byref(bits), _stream(stream))
+        ws = getattr(self, "_last_ws", None)
+        rc = lib().p2r_queue_error(_ptr(self.ws if ws is None else ws), ctypes.byref(bits), _stream(stream))
         if rc not in (_lib.P2R_OK, _lib.P2R_ERR_QUEUE):
             check(rc)
         return int(bits.value)
