@@ -196,12 +196,13 @@ def accuracy_vs_fp64(trk_ev, hit_ev, ours_ev, nb, bsize, bz, nthreads, ref_gpu_e
         cov = t[:, 6:27, :].transpose(0, 2, 1).reshape(-1, 21).astype(np.float64)
         return par, cov
 
-    def errs(out, against=None):
+    def errs(out, against=None, truth=None):
         """Quantiles of the relative errors of `out` against the FP64 oracle (or against another
         output), and the fractions of elements beyond the stated bars (1e-4 parameters, 1e-3
         covariance)."""
         par, cov = unpack(out)
-        tp, tc = (f64["par"], f64["cov"]) if against is None else unpack(against)
+        t64 = f64 if truth is None else truth
+        tp, tc = (t64["par"], t64["cov"]) if against is None else unpack(against)
         ep = np.abs(par - tp) / np.maximum(np.abs(tp), floor)
         ec = np.abs(cov - tc) / np.maximum(np.abs(tc), scale)
         q = lambda e: {"p50": float(np.quantile(e, 0.5)), "p99": float(np.quantile(e, 0.99)), "max": float(e.max())}
@@ -220,7 +221,11 @@ def accuracy_vs_fp64(trk_ev, hit_ev, ours_ev, nb, bsize, bz, nthreads, ref_gpu_e
         res["reference_cpu"] = errs(ref_out)
         res["this_library_vs_reference_cpu"] = errs(ours_ev, against=ref_out)
     if ref_gpu_ev is not None:
-        res["reference_gpu_cuda_v4"] = errs(ref_gpu_ev)
+        # the reference's GPU program has its field compiled in (kfact of 3.8112 T, TBB:654): its
+        # output is compared with the FP64 oracle run at that field on the same inputs
+        f64_ref_field = Oracle().run(trk_ev, hit_ev, bsize, NLAYER, 1, 3.8112, "f64")
+        res["reference_gpu_cuda_v4"] = dict(errs(ref_gpu_ev, truth=f64_ref_field),
+                                            oracle_field="3.8112 T, the program's compiled-in kfact")
     return res
 
 
@@ -604,11 +609,12 @@ def main():
         from p2r_tests_b200 import autotune
         counts = p2r.lognormal_counts(args.uneven_events, median=2000, sigma=1.0, lo=50, hi=20000, seed=7)
         wl = {bs: p2r.uneven_workload(counts, bsize=bs, nlayer_max=25) for bs in (32, 64)}
-        tq = autotune.tune_queue(counts, bsizes=(32, 64), granularity=(1, 4, 16), threads=(64, 128),
+        tq = autotune.tune_queue(counts, bsizes=(32, 64), granularity=(1, 4, 8, 16), threads=(64, 128),
                                  stages=(4,), reps=3, use_cache=False, workloads=wl)
         w = wl[tq["bsize"]]
-        q = p2r.Queue(w, blocks_per_item=tq["blocks_per_item"], block_threads=tq["block_threads"],
-                      stages=tq["stages"])
+        qflags = p2r.FLAG_ORDER_BY_LAYERS if tq.get("order") else 0
+        q = p2r.Queue(w, blocks_per_item=tq["blocks_per_item"], block_threads=0 if qflags else tq["block_threads"],
+                      stages=tq["stages"], flags=qflags)
         qt = torch.from_numpy(w["trk"].reshape(-1)).to(dev)
         qh = torch.from_numpy(w["hit"].reshape(-1)).to(dev)
         qo = torch.empty_like(qt)
@@ -629,8 +635,8 @@ def main():
         # the same tracks ordered by layer count within each event (p2r.sort_by_layers): warps
         # of tracks with similar lengths idle less; per-track results are bit-identical
         ws_, perm = p2r.sort_by_layers(w)
-        qs = p2r.Queue(ws_, blocks_per_item=tq["blocks_per_item"], block_threads=tq["block_threads"],
-                       stages=tq["stages"])
+        qs = p2r.Queue(ws_, blocks_per_item=tq["blocks_per_item"], block_threads=0 if qflags else tq["block_threads"],
+                       stages=tq["stages"], flags=qflags)
         st_, sh_ = torch.from_numpy(ws_["trk"].reshape(-1)).to(dev), torch.from_numpy(ws_["hit"].reshape(-1)).to(dev)
         so_ = torch.empty_like(st_)
         qs.capture(st_, sh_, so_)
@@ -651,9 +657,16 @@ def main():
                               "[50, 20000], layers/track uniform 10..25, chained",
                   "tracks": int(counts.sum()), "updates": w["updates"], "bsize": tq["bsize"],
                   "blocks_per_item": tq["blocks_per_item"], "block_threads": tq["block_threads"],
-                  "stages": tq["stages"], "ms_per_step": gms, "updates_per_s": w["updates"] / (gms / 1e3),
+                  "stages": tq["stages"], "ordered_in_launch": bool(qflags),
+                  "best_unordered": min(({"ms": x["ms"], "updates_per_s": x["updates_per_s"], "bsize": x["bsize"],
+                                          "blocks_per_item": x["blocks_per_item"], "block_threads": x["block_threads"]}
+                                         for x in tq["tried"] if not x.get("order")), key=lambda x: x["ms"],
+                                        default=None),
+                  "ms_per_step": gms, "updates_per_s": w["updates"] / (gms / 1e3),
                   "p50_event_ms": float(np.percentile(lat, 50)), "p99_event_ms": float(np.percentile(lat, 99)),
-                  "launch": "CUDA graph (queue init + one persistent kernel)", "steps": args.uneven_steps,
+                  "launch": "CUDA graph (queue init + one persistent kernel" +
+                            (", each CTA ordering its tracks by layer count in the launch)" if qflags else ")"),
+                  "steps": args.uneven_steps,
                   "autotune_candidates": len(tq["tried"]),
                   "sorted_by_layer_count": {"ms_per_step": sms, "updates_per_s": w["updates"] / (sms / 1e3),
                                             "outputs_identical_per_track": same,
@@ -723,7 +736,6 @@ def main():
         b1.record(stream)
         torch.cuda.synchronize()
         bms = b0.elapsed_time(b1) / args.calib_steps
-        ev_sum = out4["grad_dr_event"].sum(0)
         # the same forward + adjoint on the tracks ordered by layer count (same workspace)
         out4s = {"grad_trk_in": None, "grad_hits": None, "workspace": out4["workspace"]}
         p2r.forward_backward(c4, t4s, h4s, dr=dr4, nlay_lane=nl4s, grad_chi2=gc4, per_event=True, out=out4s,
@@ -738,6 +750,35 @@ def main():
         bms_sorted = b0.elapsed_time(b1) / args.calib_steps
         dr_rel = float(((out4s["grad_dr"] - out4["grad_dr"]).abs().max() / out4["grad_dr"].abs().max()).item())
         del out4s, t4s, h4s, nl4s
+        # the grid path with the ordering inside the call (P2R_FLAG_ORDER_BY_LAYERS: the order is
+        # computed on the device and the kernels read each position's track through it), in a graph
+        ref_dr, ref_ev, ref_bz = (out4["grad_dr"].clone(), out4["grad_dr_event"].clone(),
+                                  out4["grad_bz_event"].clone())
+        ev_ok = bool(torch.allclose(out4["grad_dr_event"].sum(0), out4["grad_dr"], rtol=1e-10, atol=0))
+        del graph4
+        out4["workspace"] = None  # the ordered call's workspace is 4 bytes per track larger
+        torch.cuda.empty_cache()
+        c4o = dataclasses.replace(c4, flags=c4.flags | p2r.FLAG_ORDER_BY_LAYERS)
+        out4o = {"grad_trk_in": None, "grad_hits": None}
+        p2r.forward_backward(c4o, t4, h4, dr=dr4, nlay_lane=nl4, grad_chi2=gc4, per_event=True, out=out4o,
+                             ckpt_stride=ck4, stream=stream)
+        torch.cuda.synchronize()
+        graph4o = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph4o, stream=cap):
+            p2r.forward_backward(c4o, t4, h4, dr=dr4, nlay_lane=nl4, grad_chi2=gc4, per_event=True, out=out4o,
+                                 ckpt_stride=ck4, stream=cap)
+        graph4o.replay()
+        torch.cuda.synchronize()
+        b0.record(stream)
+        for _ in range(args.calib_steps):
+            graph4o.replay()
+        b1.record(stream)
+        torch.cuda.synchronize()
+        bms_ord = b0.elapsed_time(b1) / args.calib_steps
+        ord_rel = float(((out4o["grad_dr_event"] - ref_ev).abs().max() / ref_ev.abs().max()).item())
+        ws_ord = int(out4o["workspace"].numel())
+        del graph4o, out4o, out4
+        torch.cuda.empty_cache()
         # the same forward + adjoint in ONE persistent launch over the work queue (per-warp tapes,
         # the workspace bounded by the resident warps), captured in a CUDA graph; plain and with
         # each event's tracks ordered by layer count inside the launch
@@ -756,7 +797,6 @@ def main():
             b1.record(stream)
             torch.cuda.synchronize()
             qms = b0.elapsed_time(b1) / args.calib_steps
-            ref_ev, ref_bz = out4["grad_dr_event"], out4["grad_bz_event"]
             qadj[name] = {
                 "ms_per_step": qms, "ratio_vs_forward": qms / fms, "updates_per_s": upd4 / (qms / 1e3),
                 "workspace_bytes": int(oq["workspace"].numel()), "queue_errors": qa.error_bits(stream),
@@ -790,11 +830,17 @@ def main():
                                          "grad_dr_max_rel_diff_vs_unsorted": dr_rel,
                                          "how": "each event's tracks ordered by layer count (p2r.sort_by_layers_device), "
                                                 "direct calls"},
+                                     "ordered_in_call": {
+                                         "ms_per_step": bms_ord, "ratio_vs_forward": bms_ord / fms,
+                                         "workspace_bytes": ws_ord,
+                                         "grad_dr_event_max_rel_diff_vs_unordered": ord_rel,
+                                         "how": "P2R_FLAG_ORDER_BY_LAYERS: order computed on the device inside "
+                                                "the call, replayed from one CUDA graph"},
                                      "api": f"p2r_forward_backward (FP64, ckpt {ck4}), per-event grad_dr/grad_bz, "
                                             "replayed from one CUDA graph"},
-                 "per_event_sum_matches_total": bool(torch.allclose(ev_sum, out4["grad_dr"], rtol=1e-10, atol=0)),
+                 "per_event_sum_matches_total": ev_ok,
                  "steps": args.calib_steps}
-        del graph4, out4, t4, h4, nl4, gc4
+        del t4, h4, nl4, gc4
 
     # end to end through the host-buffer C-ABI call: H2D + kernels + D2H every step
     h_trk = torch.from_numpy(trk.reshape(-1)).pin_memory().numpy()

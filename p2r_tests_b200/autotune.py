@@ -16,7 +16,7 @@ from pathlib import Path
 
 import numpy as np
 
-from ._lib import CTuneResult, check, lib
+from ._lib import FLAG_ORDER_BY_LAYERS, CTuneResult, check, lib
 from .api import Config, HIT_WORDS, TRK_WORDS, _stream
 
 
@@ -97,14 +97,18 @@ def tune_forward(cfg: Config, trk: np.ndarray, hit: np.ndarray, bsizes=(32, 64, 
 
 
 def tune_queue(ntrk_event, bsizes=(32, 64, 128), granularity=(1, 2, 4, 8, 16), threads=(64, 128), stages=(4,),
-               reps: int = 5, nlayer_max: int = 25, use_cache: bool = True, workloads: dict | None = None) -> dict:
-    """Best (bsize, blocks_per_item, block_threads, stages) for the persistent queue launch."""
+               reps: int = 5, nlayer_max: int = 25, use_cache: bool = True, workloads: dict | None = None,
+               order=(False, True)) -> dict:
+    """Best (bsize, blocks_per_item, block_threads, stages, order) for the persistent queue launch.
+    order True: each CTA orders its tracks by layer count (P2R_FLAG_ORDER_BY_LAYERS; 256 threads
+    per CTA, so block_threads is not varied there)."""
     import torch
 
     from .uneven import Queue, uneven_workload
     counts = np.asarray(ntrk_event, np.int64)
     sig = f"nevts={len(counts)}|ntr={int(counts.sum())}|median={int(np.median(counts))}|nlay={nlayer_max}"
-    key = f"{_gpu_name()}|queue|{sig}|space={tuple(bsizes)}x{tuple(granularity)}x{tuple(threads)}x{tuple(stages)}"
+    key = (f"{_gpu_name()}|queue|{sig}|space={tuple(bsizes)}x{tuple(granularity)}x{tuple(threads)}x{tuple(stages)}"
+           f"x{tuple(order)}")
     if use_cache and key in _load_cache():
         return _load_cache()[key]
     results = []
@@ -113,23 +117,24 @@ def tune_queue(ntrk_event, bsizes=(32, 64, 128), granularity=(1, 2, 4, 8, 16), t
         dt = torch.from_numpy(w["trk"].reshape(-1)).cuda()
         dh = torch.from_numpy(w["hit"].reshape(-1)).cuda()
         do = torch.empty_like(dt)
-        for g in granularity:
-            for nt in threads:
-                for st in stages:
-                    q = Queue(w, blocks_per_item=g, block_threads=nt, stages=st)
-                    q.run(dt, dh, do)
-                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    e0.record()
-                    for _ in range(reps):
-                        q.run(dt, dh, do)
-                    e1.record()
-                    torch.cuda.synchronize()
-                    ms = e0.elapsed_time(e1) / reps
-                    lat = q.event_latency_ns()
-                    results.append({"bsize": bs, "blocks_per_item": g, "block_threads": nt, "stages": st, "ms": ms,
-                                    "updates_per_s": w["updates"] / (ms / 1e3),
-                                    "p50_event_ms": float(np.percentile(lat, 50)) / 1e6,
-                                    "p99_event_ms": float(np.percentile(lat, 99)) / 1e6})
+        shapes = [(g, nt, st, False) for g in granularity for nt in threads for st in stages if False in order]
+        shapes += [(g, 256, st, True) for g in granularity for st in stages if True in order and bs <= 256]
+        for g, nt, st, ordered in shapes:
+            q = Queue(w, blocks_per_item=g, block_threads=0 if ordered else nt, stages=st,
+                      flags=FLAG_ORDER_BY_LAYERS if ordered else 0)
+            q.run(dt, dh, do)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                q.run(dt, dh, do)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            lat = q.event_latency_ns()
+            results.append({"bsize": bs, "blocks_per_item": g, "block_threads": nt, "stages": st,
+                            "order": ordered, "ms": ms, "updates_per_s": w["updates"] / (ms / 1e3),
+                            "p50_event_ms": float(np.percentile(lat, 50)) / 1e6,
+                            "p99_event_ms": float(np.percentile(lat, 99)) / 1e6})
         del dt, dh, do
     best = min(results, key=lambda x: x["ms"])
     out = {**best, "tried": results, "when": time.strftime("%Y-%m-%dT%H:%M:%S")}

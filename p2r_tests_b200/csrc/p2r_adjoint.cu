@@ -47,6 +47,7 @@ struct AdjParams {
   float* g_trk_in;          // nullable, Matriplex
   float* g_hits;            // nullable, Matriplex
   double* partials;         // [nwarps][nlayer + 1]
+  const uint32_t* order;    // nullable: the track at each position (each event's tracks by layer count)
   long long nblocks;
   int bsize;
   int nlayer;
@@ -76,9 +77,15 @@ __global__ void __launch_bounds__(kAdjThreads) fwdbwd_kernel(AdjParams p) {
   const int bs = p.bsize;
   const int lane = threadIdx.x & 31;
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long b = g / bs;
-  const int it = (int)(g - b * bs);
-  const bool valid = b < p.nblocks;
+  long long b = g / bs;
+  int it = (int)(g - b * bs);
+  bool valid = b < p.nblocks;
+  if (valid && p.order) {  // position g holds track order[g]
+    const long long t = p.order[g];
+    valid = t < p.nblocks * bs;
+    b = valid ? t / bs : 0;
+    it = valid ? (int)(t - b * bs) : 0;
+  }
   const long long gwarp = g >> 5;
   double* wpart = p.partials + gwarp * (p.nlayer + 1);
 
@@ -301,8 +308,16 @@ struct TrackCtx {
 template <class T>
 __device__ __forceinline__ TrackCtx<T> grid_track(const AdjParams& p, T (&par)[6], T (&cov)[21], long long& g) {
   g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long b = g / p.bsize;
-  return TrackCtx<T>(p, par, cov, b, (int)(g - b * p.bsize), b < p.nblocks);
+  long long b = g / p.bsize;
+  int it = (int)(g - b * p.bsize);
+  bool valid = b < p.nblocks;
+  if (valid && p.order) {  // position g holds track order[g]; the tape stays indexed by position
+    const long long t = p.order[g];
+    valid = t < p.nblocks * p.bsize;
+    b = valid ? t / p.bsize : 0;
+    it = valid ? (int)(t - b * p.bsize) : 0;
+  }
+  return TrackCtx<T>(p, par, cov, b, it, valid);
 }
 
 template <class T>
@@ -564,6 +579,18 @@ struct QAdjParams {
   const uint32_t* order;  // nullable: track at each position, each event's tracks by layer count
 };
 
+// The two phases of a lane's slice as separate calls: the register allocator then treats each
+// phase on its own, as in the grid kernels, instead of keeping the forward's values live into the
+// reverse (fewer spills).
+__device__ __noinline__ void queue_fwd_call(const AdjParams& p, const TrackCtx<double>& c, double (&par)[6],
+                                            double (&cov)[21], const TapeRef<double>& tr) {
+  fwd_track_ck1(p, c, par, cov, tr);
+}
+__device__ __noinline__ void queue_rev_call(const AdjParams& p, const TrackCtx<double>& c,
+                                            const TapeRef<double>& tr, double* wpart) {
+  rev_track_ck1(p, c, tr, wpart);
+}
+
 __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAdjParams q) {
   __shared__ long long s_item;
   const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -601,8 +628,8 @@ __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAd
       }
       double par[6], cov[21];
       const TrackCtx<double> c(p, par, cov, b, it, valid);
-      fwd_track_ck1(p, c, par, cov, tr);
-      rev_track_ck1(p, c, tr, q.slice_partials + slice * (p.nlayer + 1));
+      queue_fwd_call(p, c, par, cov, tr);
+      queue_rev_call(p, c, tr, q.slice_partials + slice * (p.nlayer + 1));
     }
   }
 }
@@ -613,8 +640,8 @@ __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAd
 // lane's rank among equal keys comes from its warp (__match_any_sync) and the warps before it.
 constexpr int kOrderThreads = 512;
 __global__ void __launch_bounds__(kOrderThreads) order_by_layers_kernel(const int32_t* nlay, const int64_t* ev_off,
-                                                                       long long nblocks, int bsize, int nlayer,
-                                                                       uint32_t* order) {
+                                                                       long long nb_event, long long nblocks, int bsize,
+                                                                       int nlayer, uint32_t* order) {
   constexpr int kW = kOrderThreads / 32;
   __shared__ int hist[kMaxAdjLayers + 1];
   __shared__ long long base[kMaxAdjLayers + 1];
@@ -622,7 +649,8 @@ __global__ void __launch_bounds__(kOrderThreads) order_by_layers_kernel(const in
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nkeys = nlayer + 1;
   const long long e = blockIdx.x;
-  long long b0 = ev_off[e], b1 = ev_off[e + 1];
+  // event e's blocks: [ev_off[e], ev_off[e+1]), or [e nb_event, (e+1) nb_event) without offsets
+  long long b0 = ev_off ? ev_off[e] : e * nb_event, b1 = ev_off ? ev_off[e + 1] : (e + 1) * nb_event;
   b0 = b0 < 0 ? 0 : (b0 > nblocks ? nblocks : b0);
   b1 = b1 < b0 ? b0 : (b1 > nblocks ? nblocks : b1);
   const long long t0 = b0 * bsize, t1 = b1 * bsize;
@@ -718,9 +746,10 @@ namespace {
 // event_sums[nevts][nlayer+1] and double totals[nlayer+1]
 struct WsLayout {
   long long nwarps;
-  size_t partial_bytes, event_off, total_off, total_bytes;
+  size_t partial_bytes, event_off, total_off, order_off, total_bytes;
 };
 
+// With P2R_FLAG_ORDER_BY_LAYERS the track order (uint32 per track) follows the totals.
 WsLayout layout_of(const p2r_config* cfg) {
   WsLayout w;
   const long long ntr = (long long)cfg->nevts * cfg->nb * cfg->bsize;
@@ -730,6 +759,8 @@ WsLayout layout_of(const p2r_config* cfg) {
   w.event_off = (w.partial_bytes + 255) & ~(size_t)255;
   w.total_off = w.event_off + (((size_t)cfg->nevts * (cfg->nlayer + 1) * sizeof(double) + 255) & ~(size_t)255);
   w.total_bytes = w.total_off + (size_t)(cfg->nlayer + 1) * sizeof(double);
+  w.order_off = (w.total_bytes + 255) & ~(size_t)255;
+  if (cfg->flags & P2R_FLAG_ORDER_BY_LAYERS) w.total_bytes = w.order_off + (size_t)ntr * sizeof(uint32_t);
   return w;
 }
 
@@ -819,6 +850,8 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   if (cfg->mode != P2R_MODE_CHAINED) return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: only CHAINED mode has an adjoint", who);
   if (cfg->flags & P2R_FLAG_SQUASH_PHI)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_SQUASH_PHI is a forward-only option", who);
+  if ((cfg->flags & P2R_FLAG_ORDER_BY_LAYERS) && (long long)cfg->nevts * cfg->nb * cfg->bsize > (long long)UINT32_MAX)
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: ordering needs fewer than 2^32 tracks", who);
   if (cfg->nlayer > kMaxAdjLayers)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: nlayer %d exceeds %d", who, cfg->nlayer, kMaxAdjLayers);
   const long long nblocks = (long long)cfg->nevts * cfg->nb;
@@ -871,6 +904,9 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   p.g_trk_in = (float*)grad_trk_in;
   p.g_hits = (float*)grad_hits;
   p.partials = (double*)workspace;
+  // ordering only matters (and only runs) with per-track layer counts
+  const bool ordered = (cfg->flags & P2R_FLAG_ORDER_BY_LAYERS) && nlay_lane;
+  p.order = ordered ? (const uint32_t*)((char*)workspace + w.order_off) : nullptr;
   p.nblocks = nblocks;
   p.bsize = cfg->bsize;
   p.nlayer = cfg->nlayer;
@@ -882,6 +918,13 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
   if (ckpt_stride != 0 && ckpt_stride != 1 && ckpt_stride != 2 && ckpt_stride != 4 && ckpt_stride != 5 &&
       ckpt_stride != 10)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: checkpoint stride %d (use 1, 2, 4, 5 or 10)", who, ckpt_stride);
+  if (ordered) {
+    order_by_layers_kernel<<<(unsigned)cfg->nevts, kOrderThreads, 0, st>>>(nlay_lane, nullptr, cfg->nb, nblocks,
+                                                                           cfg->bsize, cfg->nlayer,
+                                                                           (uint32_t*)p.order);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: launch failed: %s", who, cudaGetErrorString(e));
+  }
   const bool fp32 = (cfg->flags & P2R_FLAG_ADJ_FP32) != 0;
   const int ck = normal_ckpt(ckpt_stride);
   const TapeLayout tl = tape_layout_of(cfg, ck, fp32 ? sizeof(float) : sizeof(double));
@@ -1183,6 +1226,7 @@ int enqueue_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hi
   p.g_trk_in = (float*)grad_trk_in;
   p.g_hits = (float*)grad_hits;
   p.partials = nullptr;
+  p.order = nullptr;  // the queue kernel reads its own order (QAdjParams)
   p.nblocks = q->nblocks;
   p.bsize = q->bsize;
   p.nlayer = q->nlayer;
@@ -1204,7 +1248,7 @@ int enqueue_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hi
     e = cudaMemsetAsync(qp.slice_partials, 0, (size_t)w.nslices * (q->nlayer + 1) * sizeof(double), st);
   if (e == cudaSuccess && qp.order && q->nblocks > 0) {
     order_by_layers_kernel<<<(unsigned)q->nevts, kOrderThreads, 0, st>>>(
-        q->nlay_lane, q->event_block_offset, q->nblocks, q->bsize, q->nlayer, (uint32_t*)qp.order);
+        q->nlay_lane, q->event_block_offset, 0, q->nblocks, q->bsize, q->nlayer, (uint32_t*)qp.order);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess && q->n_items > 0) {

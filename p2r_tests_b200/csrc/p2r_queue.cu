@@ -97,6 +97,173 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
   }
 }
 
+// ---------------------------------------------------------------- ordered variant
+// Each CTA (8 warps) runs a chunk of an item, floor(256 / bsize) blocks (at most 256 tracks), with
+// the chunk's tracks ordered by layer count: a warp's 32 lanes take tracks of similar length, so
+// few lanes idle while the longest track of the warp runs. The chunk's hits are staged layer by
+// layer for all its blocks at once (cp.async into a shared ring of STAGES layers, one barrier per
+// layer), and each lane reads its own track's 9 values from there, so global loads stay whole
+// 16-byte chunks of the Matriplex rows. Warps whose tracks are done wait at the barriers without
+// issuing. Per track the arithmetic is the masked forward's, in the same order: bit-identical
+// results. nlayer <= 64 (the ordering keys), bsize <= 256.
+constexpr int kOrdThreads = 256;
+constexpr int kOrdWarps = kOrdThreads / 32;
+constexpr int kOrdMaxKeys = 65;
+
+template <int BS, int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
+__global__ void __launch_bounds__(kOrdThreads) queue_ordered_kernel(QueueParams q) {
+  __shared__ __align__(16) float ring[STAGES * kOrdThreads * kHitWords];
+  __shared__ int s_order[kOrdThreads];
+  __shared__ int s_wcount[kOrdWarps][kOrdMaxKeys];
+  __shared__ int s_base[kOrdMaxKeys];
+  __shared__ int s_maxnl;
+  __shared__ long long s_item;
+  const FwdParams& p = q.f;
+  const int bs = BS > 0 ? BS : p.bsize;
+  const int spb = bs / 32;
+  const int cb = kOrdThreads / bs;  // blocks per chunk
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nkeys = p.nlayer + 1;
+  const unsigned lt = (1u << lane) - 1u;
+  if (tid == 0 && q.t_start) atomicMin(q.t_start, globaltimer_ns());
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(q.counter, 1);
+    __syncthreads();
+    const long long item = s_item;
+    __syncthreads();  // every thread has read s_item before thread 0 claims the next one
+    if (item >= q.n_items) break;
+    const p2r_queue_item qi = q.items[item];
+    const unsigned bad = queue_item_error(qi, q.nevts, p.nblocks, q.ev_off);
+    if (bad) {
+      if (tid == 0) atomicOr(q.error, bad);
+      continue;
+    }
+    for (int c0 = 0; c0 < qi.nblk; c0 += cb) {
+      const long long b0 = qi.block0 + c0;
+      const int nblk = min(cb, qi.nblk - c0);
+      const int ntrk = nblk * bs;
+      // ---- order the chunk's tracks: stable counting sort on key = nlayer - layers
+      const bool real = tid < ntrk;
+      int key = -1;
+      if (real) {
+        const int v = p.nlay[(b0 + tid / bs) * bs + tid % bs];
+        key = p.nlayer - min(p.nlayer, max(0, v));
+      }
+      const unsigned same = __match_any_sync(0xffffffffu, key);
+      const int rank = __popc(same & lt);
+      for (int j = lane; j < nkeys; j += 32) s_wcount[warp][j] = 0;
+      __syncwarp();
+      if (real && rank == 0) s_wcount[warp][key] = __popc(same);
+      __syncthreads();
+      if (tid == 0) {
+        int run = 0, maxnl = 0;
+        for (int k = 0; k < nkeys; ++k) {
+          int tot = 0;
+          for (int w = 0; w < kOrdWarps; ++w) tot += s_wcount[w][k];
+          if (tot > 0 && maxnl == 0) maxnl = p.nlayer - k;
+          s_base[k] = run;
+          run += tot;
+        }
+        s_maxnl = maxnl;
+      }
+      __syncthreads();
+      if (real) {
+        int pos = s_base[key] + rank;
+        for (int w = 0; w < warp; ++w) pos += s_wcount[w][key];
+        s_order[pos] = tid;
+      }
+      __syncthreads();
+      const int maxnl = s_maxnl;
+      // ---- this lane's track: the one at sorted position tid
+      const bool mine = tid < ntrk;
+      const int li = mine ? s_order[tid] : 0;
+      const int jb = li / bs, it = li - jb * bs;
+      const long long b = b0 + jb;
+      float par[6], cov[21];
+      int qq = 1, nl = 0;
+      if (mine) {
+        load_track(p.trk_in + b * (long long)(kTrkWords * bs), bs, it, par, cov, qq);
+        nl = min(p.nlayer, max(0, p.nlay[b * bs + it]));
+      }
+      const float k = (float)qq * p.kfact;
+      const float kinv = 1.f / k;
+      const int nl_warp = __reduce_max_sync(0xffffffffu, nl);
+      float chi2 = 0.f;
+      // ---- layers: the chunk's hits of layer l staged for all its blocks
+      const int nchunk16 = ntrk * kHitWords / 4;  // 16-byte chunks per layer
+      auto stage_layer = [&](int l, float* stg) {
+        for (int c = tid; c < nchunk16; c += kOrdThreads) {
+          const int j = c / (kHitWords * bs / 4), r = c - j * (kHitWords * bs / 4);
+          cp_async16(stg + j * (kHitWords * bs) + r * 4,
+                     p.hits + ((b0 + j) * (long long)p.nlayer + l) * (kHitWords * bs) + r * 4);
+        }
+      };
+#pragma unroll
+      for (int sgi = 0; sgi < STAGES - 1; ++sgi) {
+        if (sgi < maxnl) stage_layer(sgi, ring + sgi * (kOrdThreads * kHitWords));
+        cp_async_commit();
+      }
+      for (int l = 0; l < maxnl; ++l) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();  // layer l landed for every thread; layer l-1's stage is free to refill
+        const int ln = l + STAGES - 1;
+        if (ln < maxnl) stage_layer(ln, ring + (ln % STAGES) * (kOrdThreads * kHitWords));
+        cp_async_commit();
+        if (l < nl_warp) {
+          const float* st = ring + (l % STAGES) * (kOrdThreads * kHitWords) + jb * (kHitWords * bs) + it;
+          float hp[3], hc[6];
+#pragma unroll
+          for (int i = 0; i < 3; ++i) hp[i] = st[i * bs];
+#pragma unroll
+          for (int i = 0; i < 6; ++i) hc[i] = st[(3 + i) * bs];
+          if (l < nl) {
+            const float rh = hipo(hp[0], hp[1]);
+            propagate_to_r(par, cov, k, kinv, rh, par, cov);
+            chi2 += kalman_update<FP64DET, CHI2>(par, cov, hp, hc, rh);
+            if (SQUASH) par[4] = squash_phi(par[4]);
+          }
+        }
+      }
+      cp_async_wait<0>();
+      __syncthreads();  // the ring and the order are reused by the next chunk
+      if (mine) {
+        store_track(p.trk_out + b * (long long)(kTrkWords * bs), bs, it, par, cov, qq);
+        if (CHI2) p.chi2[b * bs + it] = chi2;
+      }
+      if (tid == 0) {
+        __threadfence();
+        if (atomicSub(&q.ev_remaining[qi.event], nblk * spb) == nblk * spb && q.ev_done)
+          q.ev_done[qi.event] = globaltimer_ns();
+      }
+    }
+  }
+}
+
+template <int BS, int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
+cudaError_t launch_queue_ordered_t(const QueueParams& q, int ctas_per_sm, cudaStream_t st) {
+  auto kern = queue_ordered_kernel<BS, STAGES, CHI2, FP64DET, SQUASH>;
+  int dev = 0, sms = 0, occ = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kOrdThreads, 0);
+  if (e != cudaSuccess) return e;
+  const int per_sm = ctas_per_sm > 0 ? (ctas_per_sm < occ ? ctas_per_sm : occ) : occ;
+  const long long want = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  const long long grid = want < q.n_items ? want : (q.n_items > 0 ? q.n_items : 1);
+  kern<<<(unsigned)grid, kOrdThreads, 0, st>>>(q);
+  return cudaGetLastError();
+}
+
+template <int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
+cudaError_t launch_queue_ordered_bs(const QueueParams& q, int ctas, cudaStream_t st) {
+  switch (q.f.bsize) {
+    case 32: return launch_queue_ordered_t<32, STAGES, CHI2, FP64DET, SQUASH>(q, ctas, st);
+    case 64: return launch_queue_ordered_t<64, STAGES, CHI2, FP64DET, SQUASH>(q, ctas, st);
+    case 128: return launch_queue_ordered_t<128, STAGES, CHI2, FP64DET, SQUASH>(q, ctas, st);
+    default: return launch_queue_ordered_t<0, STAGES, CHI2, FP64DET, SQUASH>(q, ctas, st);
+  }
+}
+
 template <int BS, int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
 cudaError_t launch_queue_t(const QueueParams& q, int threads, int ctas_per_sm, cudaStream_t st) {
   auto kern = queue_kernel<BS, STAGES, CHI2, FP64DET, SQUASH>;
@@ -173,8 +340,10 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
   P2rRange range(who);
   int rc = p2r_check_queue(q, who);
   if (rc) return rc;
-  if (q->flags & P2R_FLAG_ORDER_BY_LAYERS)
-    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_ORDER_BY_LAYERS is an option of the queue adjoint", who);
+  const bool ordered = (q->flags & P2R_FLAG_ORDER_BY_LAYERS) != 0;
+  if (ordered && (q->nlayer > kOrdMaxKeys - 1 || q->bsize > kOrdThreads))
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_ORDER_BY_LAYERS needs nlayer <= %d and bsize <= %d", who,
+                          kOrdMaxKeys - 1, kOrdThreads);
   const QueueWs w = queue_ws(q->nevts);
   if (!workspace || ws_bytes < w.bytes)
     return p2r_set_errorf(P2R_ERR_WORKSPACE, "%s: workspace of %zu bytes needed", who, w.bytes);
@@ -238,6 +407,18 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
     const int c = q->ctas_per_sm;
     if (qp.f.squash && !fp64) {
       e = cudaErrorNotSupported;  // rejected before launch in p2r_run_queue's checks
+    } else if (ordered) {
+#define P2R_O(S, C, F, Q) launch_queue_ordered_bs<S, C, F, Q>(qp, c, st)
+      if (qp.f.squash)
+        e = stages == 2 ? (chi2 ? P2R_O(2, true, true, true) : P2R_O(2, false, true, true))
+                        : (chi2 ? P2R_O(4, true, true, true) : P2R_O(4, false, true, true));
+      else if (stages == 2)
+        e = chi2 ? (fp64 ? P2R_O(2, true, true, false) : P2R_O(2, true, false, false))
+                 : (fp64 ? P2R_O(2, false, true, false) : P2R_O(2, false, false, false));
+      else
+        e = chi2 ? (fp64 ? P2R_O(4, true, true, false) : P2R_O(4, true, false, false))
+                 : (fp64 ? P2R_O(4, false, true, false) : P2R_O(4, false, false, false));
+#undef P2R_O
     } else if (qp.f.squash) {
       e = stages == 2 ? (chi2 ? launch_queue_bs<2, true, true, true>(qp, threads, c, st)
                               : launch_queue_bs<2, false, true, true>(qp, threads, c, st))

@@ -88,17 +88,21 @@ def small_batch(p2r):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("g,flags", [(1, 0), (4, 0), (16, 0), (4, "squash")])
+@pytest.mark.parametrize("g,flags", [(1, 0), (4, 0), (16, 0), (4, "squash"), (1, "order"), (8, "order"), (20, "order"),
+                                     (8, "order+squash")])
 def test_queue_matches_masked_forward(p2r, torch, small_batch, g, flags):
     """The persistent queue performs the masked fused forward's operations: bit-identical
-    (also with phi wrapped after every update)."""
+    (also with phi wrapped after every update, and with each CTA's tracks ordered by layer
+    count: P2R_FLAG_ORDER_BY_LAYERS)."""
     w = small_batch
-    fl = p2r.FLAG_SQUASH_PHI if flags == "squash" else 0
+    fl = (p2r.FLAG_SQUASH_PHI if "squash" in str(flags) else 0) | (p2r.FLAG_ORDER_BY_LAYERS if "order" in str(flags)
+                                                                   else 0)
     q = p2r.Queue(w, blocks_per_item=g, flags=fl)
     t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
     out = torch.empty_like(t)
     q.run(t, h, out)
-    cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"], flags=fl)
+    cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"],
+                     flags=fl & ~p2r.FLAG_ORDER_BY_LAYERS)
     ref = torch.empty_like(t)
     p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
     torch.cuda.synchronize()
@@ -198,12 +202,12 @@ def test_queue_empty_events_and_tiny(p2r, torch):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("bs", [64, 128])
-def test_queue_wide_blocks(p2r, torch, bs):
+@pytest.mark.parametrize("bs,order", [(64, False), (128, False), (64, True), (96, True), (256, True)])
+def test_queue_wide_blocks(p2r, torch, bs, order):
     w = p2r.uneven_workload(p2r.lognormal_counts(6, median=300, lo=5, hi=2000, seed=5), bsize=bs)
     t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
     out, ref = torch.empty_like(t), torch.empty_like(t)
-    p2r.Queue(w, blocks_per_item=2).run(t, h, out)
+    p2r.Queue(w, blocks_per_item=2, flags=p2r.FLAG_ORDER_BY_LAYERS if order else 0).run(t, h, out)
     cfg = p2r.Config(bsize=bs, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"])
     p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
     torch.cuda.synchronize()
