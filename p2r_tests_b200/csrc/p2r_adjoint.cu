@@ -579,18 +579,6 @@ struct QAdjParams {
   const uint32_t* order;  // nullable: track at each position, each event's tracks by layer count
 };
 
-// The two phases of a lane's slice as separate calls: the register allocator then treats each
-// phase on its own, as in the grid kernels, instead of keeping the forward's values live into the
-// reverse (fewer spills).
-__device__ __noinline__ void queue_fwd_call(const AdjParams& p, const TrackCtx<double>& c, double (&par)[6],
-                                            double (&cov)[21], const TapeRef<double>& tr) {
-  fwd_track_ck1(p, c, par, cov, tr);
-}
-__device__ __noinline__ void queue_rev_call(const AdjParams& p, const TrackCtx<double>& c,
-                                            const TapeRef<double>& tr, double* wpart) {
-  rev_track_ck1(p, c, tr, wpart);
-}
-
 __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAdjParams q) {
   __shared__ long long s_item;
   const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -628,8 +616,8 @@ __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAd
       }
       double par[6], cov[21];
       const TrackCtx<double> c(p, par, cov, b, it, valid);
-      queue_fwd_call(p, c, par, cov, tr);
-      queue_rev_call(p, c, tr, q.slice_partials + slice * (p.nlayer + 1));
+      fwd_track_ck1(p, c, par, cov, tr);
+      rev_track_ck1(p, c, tr, q.slice_partials + slice * (p.nlayer + 1));
     }
   }
 }

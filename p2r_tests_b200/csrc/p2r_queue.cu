@@ -98,33 +98,36 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
 }
 
 // ---------------------------------------------------------------- ordered variant
-// Each CTA (8 warps) runs a chunk of an item, floor(256 / bsize) blocks (at most 256 tracks), with
-// the chunk's tracks ordered by layer count: a warp's 32 lanes take tracks of similar length, so
-// few lanes idle while the longest track of the warp runs. The chunk's hits are staged layer by
-// layer for all its blocks at once (cp.async into a shared ring of STAGES layers, one barrier per
-// layer), and each lane reads its own track's 9 values from there, so global loads stay whole
-// 16-byte chunks of the Matriplex rows. Warps whose tracks are done wait at the barriers without
-// issuing. Per track the arithmetic is the masked forward's, in the same order: bit-identical
-// results. nlayer <= 64 (the ordering keys), bsize <= 256.
+// Each CTA (8 warps) takes a chunk of an item, floor(512 / bsize) blocks (at most 512 tracks), and
+// orders the chunk's tracks by layer count (a stable counting sort in shared memory), so that the
+// 32 lanes of a warp run tracks of similar length and few lanes idle while a warp's longest track
+// runs. The ordered tracks form 16 groups of 32; warp w runs group w and then group 15 - w, one
+// long and one short group, so the 8 warps finish the chunk at about the same time and the CTA
+// rarely holds a lone warp. A lane reads its own track's hits straight from the Matriplex rows
+// (the chunk's blocks are shared by the CTA's warps through L1), the next layer's hits loaded
+// while the current one computes; warps synchronise only at chunk boundaries. Per track the
+// arithmetic is the masked forward's, in the same order: bit-identical results.
+// nlayer <= 64 (the ordering keys), bsize <= 512.
 constexpr int kOrdThreads = 256;
 constexpr int kOrdWarps = kOrdThreads / 32;
+constexpr int kOrdTracks = 2 * kOrdThreads;  // tracks per chunk: two groups of 32 per warp
 constexpr int kOrdMaxKeys = 65;
 
 template <int BS, int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
-__global__ void __launch_bounds__(kOrdThreads) queue_ordered_kernel(QueueParams q) {
-  __shared__ __align__(16) float ring[STAGES * kOrdThreads * kHitWords];
-  __shared__ int s_order[kOrdThreads];
+__global__ void __launch_bounds__(kOrdThreads, 3) queue_ordered_kernel(QueueParams q) {
+  __shared__ int s_order[kOrdTracks];
   __shared__ int s_wcount[kOrdWarps][kOrdMaxKeys];
   __shared__ int s_base[kOrdMaxKeys];
-  __shared__ int s_maxnl;
+  __shared__ int s_cnt[2][kOrdMaxKeys];
   __shared__ long long s_item;
   const FwdParams& p = q.f;
   const int bs = BS > 0 ? BS : p.bsize;
   const int spb = bs / 32;
-  const int cb = kOrdThreads / bs;  // blocks per chunk
+  const int cb = kOrdTracks / bs;  // blocks per chunk
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nkeys = p.nlayer + 1;
   const unsigned lt = (1u << lane) - 1u;
+  const long long lstride = (long long)kHitWords * bs;
   if (tid == 0 && q.t_start) atomicMin(q.t_start, globaltimer_ns());
   for (;;) {
     if (tid == 0) s_item = atomicAdd(q.counter, 1);
@@ -142,94 +145,93 @@ __global__ void __launch_bounds__(kOrdThreads) queue_ordered_kernel(QueueParams 
       const long long b0 = qi.block0 + c0;
       const int nblk = min(cb, qi.nblk - c0);
       const int ntrk = nblk * bs;
-      // ---- order the chunk's tracks: stable counting sort on key = nlayer - layers
-      const bool real = tid < ntrk;
-      int key = -1;
-      if (real) {
-        const int v = p.nlay[(b0 + tid / bs) * bs + tid % bs];
-        key = p.nlayer - min(p.nlayer, max(0, v));
-      }
-      const unsigned same = __match_any_sync(0xffffffffu, key);
-      const int rank = __popc(same & lt);
-      for (int j = lane; j < nkeys; j += 32) s_wcount[warp][j] = 0;
-      __syncwarp();
-      if (real && rank == 0) s_wcount[warp][key] = __popc(same);
-      __syncthreads();
-      if (tid == 0) {
-        int run = 0, maxnl = 0;
-        for (int k = 0; k < nkeys; ++k) {
-          int tot = 0;
-          for (int w = 0; w < kOrdWarps; ++w) tot += s_wcount[w][k];
-          if (tot > 0 && maxnl == 0) maxnl = p.nlayer - k;
-          s_base[k] = run;
-          run += tot;
-        }
-        s_maxnl = maxnl;
-      }
-      __syncthreads();
-      if (real) {
-        int pos = s_base[key] + rank;
-        for (int w = 0; w < warp; ++w) pos += s_wcount[w][key];
-        s_order[pos] = tid;
-      }
-      __syncthreads();
-      const int maxnl = s_maxnl;
-      // ---- this lane's track: the one at sorted position tid
-      const bool mine = tid < ntrk;
-      const int li = mine ? s_order[tid] : 0;
-      const int jb = li / bs, it = li - jb * bs;
-      const long long b = b0 + jb;
-      float par[6], cov[21];
-      int qq = 1, nl = 0;
-      if (mine) {
-        load_track(p.trk_in + b * (long long)(kTrkWords * bs), bs, it, par, cov, qq);
-        nl = min(p.nlayer, max(0, p.nlay[b * bs + it]));
-      }
-      const float k = (float)qq * p.kfact;
-      const float kinv = 1.f / k;
-      const int nl_warp = __reduce_max_sync(0xffffffffu, nl);
-      float chi2 = 0.f;
-      // ---- layers: the chunk's hits of layer l staged for all its blocks
-      const int nchunk16 = ntrk * kHitWords / 4;  // 16-byte chunks per layer
-      auto stage_layer = [&](int l, float* stg) {
-        for (int c = tid; c < nchunk16; c += kOrdThreads) {
-          const int j = c / (kHitWords * bs / 4), r = c - j * (kHitWords * bs / 4);
-          cp_async16(stg + j * (kHitWords * bs) + r * 4,
-                     p.hits + ((b0 + j) * (long long)p.nlayer + l) * (kHitWords * bs) + r * 4);
-        }
-      };
+      // ---- order the chunk's tracks: stable counting sort on key = nlayer - layers, over two
+      // passes of 256 tracks (track t = pass * 256 + tid); a track's rank among equal keys comes
+      // from its warp (__match_any_sync) and the warps before it, pass 1 after all of pass 0
+      int keyv[2], rankv[2];
 #pragma unroll
-      for (int sgi = 0; sgi < STAGES - 1; ++sgi) {
-        if (sgi < maxnl) stage_layer(sgi, ring + sgi * (kOrdThreads * kHitWords));
-        cp_async_commit();
+      for (int pass = 0; pass < 2; ++pass) {
+        const int t = pass * kOrdThreads + tid;
+        int key = -1;
+        if (t < ntrk) {
+          const int v = p.nlay[(b0 + t / bs) * bs + t % bs];
+          key = p.nlayer - min(p.nlayer, max(0, v));
+        }
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        int r = __popc(same & lt);
+        for (int j = lane; j < nkeys; j += 32) s_wcount[warp][j] = 0;
+        __syncwarp();
+        if (key >= 0 && r == 0) s_wcount[warp][key] = __popc(same);
+        __syncthreads();
+        if (key >= 0)
+          for (int w = 0; w < warp; ++w) r += s_wcount[w][key];
+        if (tid < nkeys) {
+          int tot = 0;
+          for (int w = 0; w < kOrdWarps; ++w) tot += s_wcount[w][tid];
+          s_cnt[pass][tid] = tot;
+        }
+        keyv[pass] = key;
+        rankv[pass] = r;
+        __syncthreads();  // s_wcount is reused by the next pass
       }
-      for (int l = 0; l < maxnl; ++l) {
-        cp_async_wait<STAGES - 2>();
-        __syncthreads();  // layer l landed for every thread; layer l-1's stage is free to refill
-        const int ln = l + STAGES - 1;
-        if (ln < maxnl) stage_layer(ln, ring + (ln % STAGES) * (kOrdThreads * kHitWords));
-        cp_async_commit();
-        if (l < nl_warp) {
-          const float* st = ring + (l % STAGES) * (kOrdThreads * kHitWords) + jb * (kHitWords * bs) + it;
+      if (tid == 0) {  // first position of each key
+        int run = 0;
+        for (int k = 0; k < nkeys; ++k) {
+          s_base[k] = run;
+          run += s_cnt[0][k] + s_cnt[1][k];
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int pass = 0; pass < 2; ++pass) {
+        const int key = keyv[pass];
+        if (key >= 0) s_order[s_base[key] + (pass ? s_cnt[0][key] : 0) + rankv[pass]] = pass * kOrdThreads + tid;
+      }
+      __syncthreads();
+      // ---- two ordered groups per warp: group w (long tracks), then group 15 - w (short)
+      for (int half = 0; half < 2; ++half) {
+        const int grp = half == 0 ? warp : 2 * kOrdWarps - 1 - warp;
+        const int pos = grp * 32 + lane;
+        const bool mine = pos < ntrk;
+        const int li = mine ? s_order[pos] : 0;
+        const int jb = li / bs, it = li - jb * bs;
+        const long long b = b0 + jb;
+        float par[6], cov[21];
+        int qq = 1, nl = 0;
+        if (mine) {
+          load_track(p.trk_in + b * (long long)(kTrkWords * bs), bs, it, par, cov, qq);
+          nl = min(p.nlayer, max(0, p.nlay[b * bs + it]));
+        }
+        const float k = (float)qq * p.kfact;
+        const float kinv = 1.f / k;
+        float chi2 = 0.f;
+        const float* hb = p.hits + b * (long long)p.nlayer * lstride + it;
+        float hn[9];
+        if (nl > 0) {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) hn[i] = __ldg(hb + i * bs);
+        }
+        for (int l = 0; l < nl; ++l) {
           float hp[3], hc[6];
 #pragma unroll
-          for (int i = 0; i < 3; ++i) hp[i] = st[i * bs];
+          for (int i = 0; i < 3; ++i) hp[i] = hn[i];
 #pragma unroll
-          for (int i = 0; i < 6; ++i) hc[i] = st[(3 + i) * bs];
-          if (l < nl) {
-            const float rh = hipo(hp[0], hp[1]);
-            propagate_to_r(par, cov, k, kinv, rh, par, cov);
-            chi2 += kalman_update<FP64DET, CHI2>(par, cov, hp, hc, rh);
-            if (SQUASH) par[4] = squash_phi(par[4]);
+          for (int i = 0; i < 6; ++i) hc[i] = hn[3 + i];
+          if (l + 1 < nl) {  // the next layer's hit, in flight while this layer computes
+#pragma unroll
+            for (int i = 0; i < 9; ++i) hn[i] = __ldg(hb + (l + 1) * lstride + i * bs);
           }
+          const float rh = hipo(hp[0], hp[1]);
+          propagate_to_r(par, cov, k, kinv, rh, par, cov);
+          chi2 += kalman_update<FP64DET, CHI2>(par, cov, hp, hc, rh);
+          if (SQUASH) par[4] = squash_phi(par[4]);
+        }
+        if (mine) {
+          store_track(p.trk_out + b * (long long)(kTrkWords * bs), bs, it, par, cov, qq);
+          if (CHI2) p.chi2[b * bs + it] = chi2;
         }
       }
-      cp_async_wait<0>();
-      __syncthreads();  // the ring and the order are reused by the next chunk
-      if (mine) {
-        store_track(p.trk_out + b * (long long)(kTrkWords * bs), bs, it, par, cov, qq);
-        if (CHI2) p.chi2[b * bs + it] = chi2;
-      }
+      __syncthreads();  // the order is reused by the next chunk
       if (tid == 0) {
         __threadfence();
         if (atomicSub(&q.ev_remaining[qi.event], nblk * spb) == nblk * spb && q.ev_done)
@@ -341,9 +343,9 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
   int rc = p2r_check_queue(q, who);
   if (rc) return rc;
   const bool ordered = (q->flags & P2R_FLAG_ORDER_BY_LAYERS) != 0;
-  if (ordered && (q->nlayer > kOrdMaxKeys - 1 || q->bsize > kOrdThreads))
+  if (ordered && (q->nlayer > kOrdMaxKeys - 1 || q->bsize > kOrdTracks))
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_ORDER_BY_LAYERS needs nlayer <= %d and bsize <= %d", who,
-                          kOrdMaxKeys - 1, kOrdThreads);
+                          kOrdMaxKeys - 1, kOrdTracks);
   const QueueWs w = queue_ws(q->nevts);
   if (!workspace || ws_bytes < w.bytes)
     return p2r_set_errorf(P2R_ERR_WORKSPACE, "%s: workspace of %zu bytes needed", who, w.bytes);
