@@ -622,17 +622,22 @@ __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAd
   }
 }
 
-// Each event's tracks ordered by layer count, longest first, ties in track order (a stable
-// counting sort; one CTA per event): order[pos] = the track placed at position pos of the
-// event's range. Keys nlayer - clamp(nlay, 0, nlayer) ascending; per chunk of 512 tracks each
-// lane's rank among equal keys comes from its warp (__match_any_sync) and the warps before it.
+// Tracks ordered by layer count, longest first, ties in track order, within windows of
+// kOrderWindow tracks (floor(kOrderWindow / bsize) whole blocks) of each event: order[pos] = the
+// track placed at position pos, always a track of the same window. Windows keep a warp's 32
+// tracks within a few neighbouring blocks, so the hits the lanes read one by one share cache
+// lines with the other warps of the window (ordering whole events of 1e5 tracks spread them over
+// the event and multiplied the device-memory traffic). Stable counting sort, one CTA per window:
+// keys nlayer - clamp(nlay, 0, nlayer) ascending; each lane's rank among equal keys comes from its
+// warp (__match_any_sync) and the warps before it. Grid (nevts, Y): CTA (e, y) sorts windows y,
+// y + Y, ... of event e.
 constexpr int kOrderThreads = 512;
+constexpr int kOrderWindow = 512;
 __global__ void __launch_bounds__(kOrderThreads) order_by_layers_kernel(const int32_t* nlay, const int64_t* ev_off,
                                                                        long long nb_event, long long nblocks, int bsize,
                                                                        int nlayer, uint32_t* order) {
   constexpr int kW = kOrderThreads / 32;
-  __shared__ int hist[kMaxAdjLayers + 1];
-  __shared__ long long base[kMaxAdjLayers + 1];
+  __shared__ int base[kMaxAdjLayers + 1];
   __shared__ int wcount[kW][kMaxAdjLayers + 1];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nkeys = nlayer + 1;
@@ -641,47 +646,64 @@ __global__ void __launch_bounds__(kOrderThreads) order_by_layers_kernel(const in
   long long b0 = ev_off ? ev_off[e] : e * nb_event, b1 = ev_off ? ev_off[e + 1] : (e + 1) * nb_event;
   b0 = b0 < 0 ? 0 : (b0 > nblocks ? nblocks : b0);
   b1 = b1 < b0 ? b0 : (b1 > nblocks ? nblocks : b1);
-  const long long t0 = b0 * bsize, t1 = b1 * bsize;
-  auto key = [&](long long t) {
-    const int v = nlay[t];
-    return nlayer - (v < 0 ? 0 : (v > nlayer ? nlayer : v));
-  };
-  for (int k = tid; k < nkeys; k += kOrderThreads) hist[k] = 0;
-  __syncthreads();
-  for (long long t = t0 + tid; t < t1; t += kOrderThreads) atomicAdd(&hist[key(t)], 1);
-  __syncthreads();
-  if (tid == 0) {
-    long long run = t0;
-    for (int k = 0; k < nkeys; ++k) {
-      base[k] = run;
-      run += hist[k];
-    }
-  }
-  __syncthreads();
+  const long long wb = kOrderWindow / bsize > 0 ? kOrderWindow / bsize : 1;  // blocks per window
+  const long long nwin = (b1 - b0 + wb - 1) / wb;
   const unsigned lt = (1u << lane) - 1u;
-  for (long long c = t0; c < t1; c += kOrderThreads) {
-    const long long t = c + tid;
-    const bool valid = t < t1;
-    const int k = valid ? key(t) : -1;
-    const unsigned same = __match_any_sync(0xffffffffu, k);
-    const int rank = __popc(same & lt);
-    for (int j = lane; j < nkeys; j += 32) wcount[warp][j] = 0;
-    __syncwarp();
-    if (valid && rank == 0) wcount[warp][k] = __popc(same);
+  for (long long wi = blockIdx.y; wi < nwin; wi += gridDim.y) {
+    const long long t0 = (b0 + wi * wb) * bsize;
+    const long long t1 = (b0 + wi * wb + wb < b1 ? b0 + wi * wb + wb : b1) * bsize;
+    // the window holds at most kOrderThreads tracks when bsize <= kOrderWindow; larger blocks
+    // make a one-block window sorted in several chunks
+    for (int k = tid; k < nkeys; k += kOrderThreads) base[k] = 0;
     __syncthreads();
-    if (valid) {
-      long long pre = base[k] + rank;
-      for (int w = 0; w < warp; ++w) pre += wcount[w][k];
-      order[pre] = (uint32_t)t;
+    for (long long t = t0 + tid; t < t1; t += kOrderThreads) {
+      const int v = nlay[t];
+      atomicAdd(&base[nlayer - (v < 0 ? 0 : (v > nlayer ? nlayer : v))], 1);
     }
     __syncthreads();
-    for (int j = tid; j < nkeys; j += kOrderThreads) {
-      long long add = 0;
-      for (int w = 0; w < kW; ++w) add += wcount[w][j];
-      base[j] += add;
+    if (tid == 0) {
+      int run = 0;
+      for (int k = 0; k < nkeys; ++k) {
+        const int c = base[k];
+        base[k] = run;
+        run += c;
+      }
     }
     __syncthreads();
+    for (long long c = t0; c < t1; c += kOrderThreads) {
+      const long long t = c + tid;
+      const bool valid = t < t1;
+      int k = -1;
+      if (valid) {
+        const int v = nlay[t];
+        k = nlayer - (v < 0 ? 0 : (v > nlayer ? nlayer : v));
+      }
+      const unsigned same = __match_any_sync(0xffffffffu, k);
+      const int rank = __popc(same & lt);
+      for (int j = lane; j < nkeys; j += 32) wcount[warp][j] = 0;
+      __syncwarp();
+      if (valid && rank == 0) wcount[warp][k] = __popc(same);
+      __syncthreads();
+      if (valid) {
+        long long pre = t0 + base[k] + rank;
+        for (int w = 0; w < warp; ++w) pre += wcount[w][k];
+        order[pre] = (uint32_t)t;
+      }
+      __syncthreads();
+      for (int j = tid; j < nkeys; j += kOrderThreads) {
+        int add = 0;
+        for (int w = 0; w < kW; ++w) add += wcount[w][j];
+        base[j] += add;
+      }
+      __syncthreads();
+    }
   }
+}
+
+// Grid of order_by_layers_kernel: one row per event, enough CTAs per event to cover ~4 per SM.
+inline dim3 order_grid(long long nevts) {
+  const long long y = nevts >= 1184 ? 1 : (1184 + nevts - 1) / nevts;
+  return dim3((unsigned)nevts, (unsigned)(y > 65535 ? 65535 : y));
 }
 
 // Sums per-warp partials [nwarps][nout] in a fixed order, in double. Block (e, j) sums
@@ -907,7 +929,7 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
       ckpt_stride != 10)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: checkpoint stride %d (use 1, 2, 4, 5 or 10)", who, ckpt_stride);
   if (ordered) {
-    order_by_layers_kernel<<<(unsigned)cfg->nevts, kOrderThreads, 0, st>>>(nlay_lane, nullptr, cfg->nb, nblocks,
+    order_by_layers_kernel<<<order_grid(cfg->nevts), kOrderThreads, 0, st>>>(nlay_lane, nullptr, cfg->nb, nblocks,
                                                                            cfg->bsize, cfg->nlayer,
                                                                            (uint32_t*)p.order);
     e = cudaGetLastError();
@@ -1235,7 +1257,7 @@ int enqueue_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hi
   if (e == cudaSuccess && w.nslices > 0)
     e = cudaMemsetAsync(qp.slice_partials, 0, (size_t)w.nslices * (q->nlayer + 1) * sizeof(double), st);
   if (e == cudaSuccess && qp.order && q->nblocks > 0) {
-    order_by_layers_kernel<<<(unsigned)q->nevts, kOrderThreads, 0, st>>>(
+    order_by_layers_kernel<<<order_grid(q->nevts), kOrderThreads, 0, st>>>(
         q->nlay_lane, q->event_block_offset, 0, q->nblocks, q->bsize, q->nlayer, (uint32_t*)qp.order);
     e = cudaGetLastError();
   }

@@ -16,7 +16,8 @@ Tolerances (the stated bar):  PAR_RTOL = 1e-4, COV_RTOL = 1e-3
   element-wise max for: single-layer steps (propagateToR, KalmanUpdate), the restart
   driver, and every step along a chained run (reference state in, one step, compare);
   for the chained end-to-end output the FP32 chain is ill-conditioned (the reference
-  itself is up to 4e-3 / 0.6 away from FP64), so there the test requires
+  itself is 3e-3 away from FP64 at the 99th percentile of covariance elements, 3.3 % of them
+  beyond COV_RTOL, and up to 0.13 on its tail), so there the test requires
   (a) the 99th percentile within PAR_RTOL / CHAIN_COV_P99 and
   (b) accuracy parity: every error quantile of the GPU against the FP64 oracle within
       ACC_FACTOR of the reference's own error quantile against the FP64 oracle.
@@ -35,7 +36,7 @@ import numpy as np
 
 PAR_RTOL = 1e-4
 COV_RTOL = 1e-3
-CHAIN_COV_P99 = 1e-2
+CHAIN_COV_P99 = 5e-3
 ACC_FACTOR = 2.0
 ACC_QUANTILES = (0.5, 0.9, 0.99, 0.999)
 STEP_ACC = 2.0
