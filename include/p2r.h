@@ -63,9 +63,10 @@ typedef enum p2r_mode { P2R_MODE_RESTART = 0, P2R_MODE_CHAINED = 1 } p2r_mode;
                                     leaves commented out (squashPhiMPlex, TBB:635); forward entry points,
                                     with the FP64 determinant (not with P2R_FLAG_FP32_DET) */
 #define P2R_FLAG_ORDER_BY_LAYERS 0x10u /* with per-track layer counts: inside the launch, order each
-                                    event's tracks by layer count (longest first, ties in track order)
-                                    within windows of 512 tracks (whole blocks) of the event, so a
-                                    warp's lanes run tracks of similar length from nearby blocks. Outputs stay at each track's own position and every
+                                    event's tracks by layer count (longest first, ties in track order),
+                                    so a warp's lanes run tracks of similar length: within windows of
+                                    512 tracks (whole blocks) for p2r_forward_backward and the forward
+                                    queue, over whole events for the queue adjoint. Outputs stay at each track's own position and every
                                     track's result is the same arithmetic; shared gradient sums are
                                     added in the new grouping. p2r_forward_backward (cfg.flags; uses
                                     4 bytes of workspace per track), the queue adjoint and the forward
@@ -303,7 +304,7 @@ int p2r_forward_backward_noalloc(const p2r_config* cfg, const void* trk_in, cons
  * slice, then per event, then in total): deterministic. Work items are checked on the device
  * (p2r_queue_error reads the result from this workspace too; bit 16: a track-order entry outside
  * the batch, which overlapping event ranges can cause). q->flags: 0 or P2R_FLAG_ORDER_BY_LAYERS
- * (the ordering runs inside the launch: a stable counting sort per 512-track window); other flags are
+ * (the ordering runs inside the launch: a stable counting sort per event); other flags are
  * rejected (P2R_ERR_UNSUPPORTED). nlayer <= 64, bsize a multiple of 32. */
 size_t p2r_queue_adjoint_workspace_size(const p2r_queue* q);
 int p2r_run_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hits, const float* dr, void* trk_out,

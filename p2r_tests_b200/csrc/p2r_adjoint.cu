@@ -623,19 +623,21 @@ __global__ void __launch_bounds__(kAdjThreads) queue_adj_kernel(AdjParams p, QAd
 }
 
 // Tracks ordered by layer count, longest first, ties in track order, within windows of
-// kOrderWindow tracks (floor(kOrderWindow / bsize) whole blocks) of each event: order[pos] = the
-// track placed at position pos, always a track of the same window. Windows keep a warp's 32
-// tracks within a few neighbouring blocks, so the hits the lanes read one by one share cache
-// lines with the other warps of the window (ordering whole events of 1e5 tracks spread them over
-// the event and multiplied the device-memory traffic). Stable counting sort, one CTA per window:
-// keys nlayer - clamp(nlay, 0, nlayer) ascending; each lane's rank among equal keys comes from its
-// warp (__match_any_sync) and the warps before it. Grid (nevts, Y): CTA (e, y) sorts windows y,
-// y + Y, ... of event e.
+// win_blocks blocks of each event (win_blocks <= 0: whole events): order[pos] = the track placed
+// at position pos, always a track of the same window. Small windows keep a warp's 32 tracks
+// within a few neighbouring blocks, so the hits the lanes read one by one share cache lines with
+// the other warps of the window; whole events give the most uniform lengths per warp. Measured on
+// the 40-layer calibration workload: the grid adjoint is faster with windows of 512 tracks
+// (kOrderWindow), the persistent queue adjoint with whole events. Stable counting sort, one CTA
+// per window: keys nlayer - clamp(nlay, 0, nlayer) ascending; each lane's rank among equal keys
+// comes from its warp (__match_any_sync) and the warps before it. Grid (nevts, Y): CTA (e, y)
+// sorts windows y, y + Y, ... of event e.
 constexpr int kOrderThreads = 512;
 constexpr int kOrderWindow = 512;
 __global__ void __launch_bounds__(kOrderThreads) order_by_layers_kernel(const int32_t* nlay, const int64_t* ev_off,
                                                                        long long nb_event, long long nblocks, int bsize,
-                                                                       int nlayer, uint32_t* order) {
+                                                                       int nlayer, long long win_blocks,
+                                                                       uint32_t* order) {
   constexpr int kW = kOrderThreads / 32;
   __shared__ int base[kMaxAdjLayers + 1];
   __shared__ int wcount[kW][kMaxAdjLayers + 1];
@@ -646,7 +648,8 @@ __global__ void __launch_bounds__(kOrderThreads) order_by_layers_kernel(const in
   long long b0 = ev_off ? ev_off[e] : e * nb_event, b1 = ev_off ? ev_off[e + 1] : (e + 1) * nb_event;
   b0 = b0 < 0 ? 0 : (b0 > nblocks ? nblocks : b0);
   b1 = b1 < b0 ? b0 : (b1 > nblocks ? nblocks : b1);
-  const long long wb = kOrderWindow / bsize > 0 ? kOrderWindow / bsize : 1;  // blocks per window
+  // blocks per window (win_blocks <= 0: the whole event is one window)
+  const long long wb = win_blocks > 0 ? win_blocks : (b1 - b0 > 0 ? b1 - b0 : 1);
   const long long nwin = (b1 - b0 + wb - 1) / wb;
   const unsigned lt = (1u << lane) - 1u;
   for (long long wi = blockIdx.y; wi < nwin; wi += gridDim.y) {
@@ -929,8 +932,9 @@ int p2r_forward_backward(const p2r_config* cfg, const void* trk_in, const void* 
       ckpt_stride != 10)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: checkpoint stride %d (use 1, 2, 4, 5 or 10)", who, ckpt_stride);
   if (ordered) {
+    const long long win = kOrderWindow / cfg->bsize > 0 ? kOrderWindow / cfg->bsize : 1;
     order_by_layers_kernel<<<order_grid(cfg->nevts), kOrderThreads, 0, st>>>(nlay_lane, nullptr, cfg->nb, nblocks,
-                                                                           cfg->bsize, cfg->nlayer,
+                                                                           cfg->bsize, cfg->nlayer, win,
                                                                            (uint32_t*)p.order);
     e = cudaGetLastError();
     if (e != cudaSuccess) return p2r_set_errorf(P2R_ERR_CUDA, "%s: launch failed: %s", who, cudaGetErrorString(e));
@@ -1258,7 +1262,7 @@ int enqueue_queue_adjoint(const p2r_queue* q, const void* trk_in, const void* hi
     e = cudaMemsetAsync(qp.slice_partials, 0, (size_t)w.nslices * (q->nlayer + 1) * sizeof(double), st);
   if (e == cudaSuccess && qp.order && q->nblocks > 0) {
     order_by_layers_kernel<<<order_grid(q->nevts), kOrderThreads, 0, st>>>(
-        q->nlay_lane, q->event_block_offset, 0, q->nblocks, q->bsize, q->nlayer, (uint32_t*)qp.order);
+        q->nlay_lane, q->event_block_offset, 0, q->nblocks, q->bsize, q->nlayer, 0, (uint32_t*)qp.order);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess && q->n_items > 0) {

@@ -246,42 +246,40 @@ P2R_UNROLL
   for (int i = 0; i < 6; ++i)
 P2R_UNROLL
     for (int j = 0; j < 6; ++j) S[i][j] = i == j ? T(2) * cb_out[S6(i, i)] : cb_out[S6(i, j)];
-  // W = S J, M = J^T W
-  T W[6][6];
-P2R_UNROLL
-  for (int a = 0; a < 6; ++a) {
-    W[a][0] = S[a][0] * t.J00 + S[a][1] * t.J10 + S[a][2] * t.J20 + S[a][4] * t.J40;
-    W[a][1] = S[a][0] * t.J01 + S[a][1] * t.J11 + S[a][2] * t.J21 + S[a][4] * t.J41;
-    W[a][2] = S[a][2];
-    W[a][3] = S[a][0] * t.J03 + S[a][1] * t.J13 + S[a][2] * t.J23 + S[a][3] + S[a][4] * t.J43;
-    W[a][4] = S[a][0] * t.J04 + S[a][1] * t.J14 + S[a][2] * t.J24 + S[a][4] * t.J44;
-    W[a][5] = S[a][2] * t.J25 + S[a][5];
-  }
+  // W = S J, column by column: column j gives column j of M = J^T W (into cb_in) and its share
+  // of Jbar = W C, Jbar_ab += W_aj C_jb, at the non-trivial entries of J. W is never held whole
+  // (the same operations in the same order as forming W first: J-bar sums over j = 0..5).
+  T J00b = 0, J01b = 0, J03b = 0, J04b = 0, J10b = 0, J11b = 0, J13b = 0, J14b = 0;
+  T J20b = 0, J21b = 0, J23b = 0, J24b = 0, J25b = 0, J40b = 0, J41b = 0, J43b = 0, J44b = 0;
 P2R_UNROLL
   for (int j = 0; j < 6; ++j) {
+    P2R_PREC_REGION(covrev);
+    T w[6];
+P2R_UNROLL
+    for (int a = 0; a < 6; ++a) {
+      if (j == 0) w[a] = S[a][0] * t.J00 + S[a][1] * t.J10 + S[a][2] * t.J20 + S[a][4] * t.J40;
+      if (j == 1) w[a] = S[a][0] * t.J01 + S[a][1] * t.J11 + S[a][2] * t.J21 + S[a][4] * t.J41;
+      if (j == 2) w[a] = S[a][2];
+      if (j == 3) w[a] = S[a][0] * t.J03 + S[a][1] * t.J13 + S[a][2] * t.J23 + S[a][3] + S[a][4] * t.J43;
+      if (j == 4) w[a] = S[a][0] * t.J04 + S[a][1] * t.J14 + S[a][2] * t.J24 + S[a][4] * t.J44;
+      if (j == 5) w[a] = S[a][2] * t.J25 + S[a][5];
+    }
     T M[6];
-    M[0] = t.J00 * W[0][j] + t.J10 * W[1][j] + t.J20 * W[2][j] + t.J40 * W[4][j];
-    M[1] = t.J01 * W[0][j] + t.J11 * W[1][j] + t.J21 * W[2][j] + t.J41 * W[4][j];
-    M[2] = W[2][j];
-    M[3] = t.J03 * W[0][j] + t.J13 * W[1][j] + t.J23 * W[2][j] + W[3][j] + t.J43 * W[4][j];
-    M[4] = t.J04 * W[0][j] + t.J14 * W[1][j] + t.J24 * W[2][j] + t.J44 * W[4][j];
-    M[5] = t.J25 * W[2][j] + W[5][j];
+    M[0] = t.J00 * w[0] + t.J10 * w[1] + t.J20 * w[2] + t.J40 * w[4];
+    M[1] = t.J01 * w[0] + t.J11 * w[1] + t.J21 * w[2] + t.J41 * w[4];
+    M[2] = w[2];
+    M[3] = t.J03 * w[0] + t.J13 * w[1] + t.J23 * w[2] + w[3] + t.J43 * w[4];
+    M[4] = t.J04 * w[0] + t.J14 * w[1] + t.J24 * w[2] + t.J44 * w[4];
+    M[5] = t.J25 * w[2] + w[5];
 P2R_UNROLL
     for (int i = j; i < 6; ++i) cb_in[S6(i, j)] = i == j ? T(0.5f) * M[i] : M[i];
+    P2R_PREC_REGION(jbar);
+    const T c0 = ic[S6(j, 0)], c1 = ic[S6(j, 1)], c3 = ic[S6(j, 3)], c4 = ic[S6(j, 4)], c5 = ic[S6(j, 5)];
+    J00b += w[0] * c0; J01b += w[0] * c1; J03b += w[0] * c3; J04b += w[0] * c4;
+    J10b += w[1] * c0; J11b += w[1] * c1; J13b += w[1] * c3; J14b += w[1] * c4;
+    J20b += w[2] * c0; J21b += w[2] * c1; J23b += w[2] * c3; J24b += w[2] * c4; J25b += w[2] * c5;
+    J40b += w[4] * c0; J41b += w[4] * c1; J43b += w[4] * c3; J44b += w[4] * c4;
   }
-
-  P2R_PREC_REGION(jbar);
-  // Jbar = W C at the non-trivial entries of J
-  auto WC = [&](int a, int b) {
-    T s = 0;
-P2R_UNROLL
-    for (int c = 0; c < 6; ++c) s += W[a][c] * ic[S6(c, b)];
-    return s;
-  };
-  const T J00b = WC(0, 0), J01b = WC(0, 1), J03b = WC(0, 3), J04b = WC(0, 4);
-  const T J10b = WC(1, 0), J11b = WC(1, 1), J13b = WC(1, 3), J14b = WC(1, 4);
-  const T J20b = WC(2, 0), J21b = WC(2, 1), J23b = WC(2, 3), J24b = WC(2, 4), J25b = WC(2, 5);
-  const T J40b = WC(4, 0), J41b = WC(4, 1), J43b = WC(4, 3), J44b = WC(4, 4);
 
   P2R_PREC_REGION(jent);
   // ---- Jacobian entries -> their inputs

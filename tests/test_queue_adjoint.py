@@ -56,12 +56,12 @@ def check_per_track(got, ref, what, tol=1e-10):
 
 
 def windowed_order(w, window=512):
-    """The library's track order: within windows of floor(window / bsize) blocks of each event,
-    tracks by layer count, longest first, ties in track order."""
+    """The library's track order: within windows of floor(window / bsize) blocks of each event
+    (window 0: whole events), tracks by layer count, longest first, ties in track order."""
     bs = w["bsize"]
     off = np.asarray(w["event_block_offset"], np.int64)
     nl = np.clip(np.asarray(w["nlay_lane"]), 0, w["nlayer"])
-    wb = max(1, window // bs)
+    wb = max(1, window // bs) if window > 0 else max(1, int(np.diff(off).max(initial=1)))
     perm = np.arange(w["nblocks"] * bs)
     for e in range(len(off) - 1):
         for b in range(off[e], off[e + 1], wb):
@@ -234,7 +234,7 @@ def test_queue_adjoint_rejects_options(p2r):
 @pytest.mark.gpu
 def test_queue_adjoint_ordered_by_layers(p2r, torch, uneven):
     """P2R_FLAG_ORDER_BY_LAYERS: the launch orders each event's tracks by layer count on the
-    device, within windows of 512 tracks (the order equals windowed_order's), every output stays
+    device, over whole events (the order equals windowed_order's), every output stays
     at its track's position and per-track results equal the unordered launch's; the shared sums
     are added in the new grouping (equal to 1e-9)."""
     w = uneven
@@ -253,7 +253,7 @@ def test_queue_adjoint_ordered_by_layers(p2r, torch, uneven):
     order_off = a256(order_off + nout * 8)
     ntr = w["nblocks"] * 32
     order = got["workspace"][order_off:order_off + 4 * ntr].cpu().numpy().view(np.uint32)
-    assert np.array_equal(order.astype(np.int64), windowed_order(w))
+    assert np.array_equal(order.astype(np.int64), windowed_order(w, window=0))
     check_per_track(got, plain, "ordered", tol=0.0)
     for k in ("grad_dr", "grad_bz", "grad_dr_event", "grad_bz_event"):
         a, b = got[k].cpu().numpy(), plain[k].cpu().numpy()
