@@ -613,7 +613,7 @@ def main():
                                  stages=(4,), reps=3, use_cache=False, workloads=wl)
         w = wl[tq["bsize"]]
         qflags = p2r.FLAG_ORDER_BY_LAYERS if tq.get("order") else 0
-        q = p2r.Queue(w, blocks_per_item=tq["blocks_per_item"], block_threads=0 if qflags else tq["block_threads"],
+        q = p2r.Queue(w, blocks_per_item=tq["blocks_per_item"], block_threads=tq["block_threads"],
                       stages=tq["stages"], flags=qflags)
         qt = torch.from_numpy(w["trk"].reshape(-1)).to(dev)
         qh = torch.from_numpy(w["hit"].reshape(-1)).to(dev)
@@ -635,7 +635,7 @@ def main():
         # the same tracks ordered by layer count within each event (p2r.sort_by_layers): warps
         # of tracks with similar lengths idle less; per-track results are bit-identical
         ws_, perm = p2r.sort_by_layers(w)
-        qs = p2r.Queue(ws_, blocks_per_item=tq["blocks_per_item"], block_threads=0 if qflags else tq["block_threads"],
+        qs = p2r.Queue(ws_, blocks_per_item=tq["blocks_per_item"], block_threads=tq["block_threads"],
                        stages=tq["stages"], flags=qflags)
         st_, sh_ = torch.from_numpy(ws_["trk"].reshape(-1)).to(dev), torch.from_numpy(ws_["hit"].reshape(-1)).to(dev)
         so_ = torch.empty_like(st_)

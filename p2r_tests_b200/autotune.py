@@ -100,8 +100,8 @@ def tune_queue(ntrk_event, bsizes=(32, 64, 128), granularity=(1, 2, 4, 8, 16), t
                reps: int = 5, nlayer_max: int = 25, use_cache: bool = True, workloads: dict | None = None,
                order=(False, True)) -> dict:
     """Best (bsize, blocks_per_item, block_threads, stages, order) for the persistent queue launch.
-    order True: each CTA orders its tracks by layer count (P2R_FLAG_ORDER_BY_LAYERS; 256 threads
-    per CTA, so block_threads is not varied there)."""
+    order True: each CTA orders its tracks by layer count (P2R_FLAG_ORDER_BY_LAYERS; block_threads
+    0 = 8 warps per CTA or 128 = 4 warps, the hit-staging depth does not apply)."""
     import torch
 
     from .uneven import Queue, uneven_workload
@@ -118,9 +118,11 @@ def tune_queue(ntrk_event, bsizes=(32, 64, 128), granularity=(1, 2, 4, 8, 16), t
         dh = torch.from_numpy(w["hit"].reshape(-1)).cuda()
         do = torch.empty_like(dt)
         shapes = [(g, nt, st, False) for g in granularity for nt in threads for st in stages if False in order]
-        shapes += [(g, 256, st, True) for g in granularity for st in stages if True in order and bs <= 256]
+        # ordered: 8 warps per CTA (block_threads 0, chunks of 512 tracks) or 4 (128, 256 tracks)
+        shapes += [(g, nt, st, True) for g in granularity for nt in (0, 128) for st in stages[:1]
+                   if True in order and bs <= 2 * (nt or 256)]
         for g, nt, st, ordered in shapes:
-            q = Queue(w, blocks_per_item=g, block_threads=0 if ordered else nt, stages=st,
+            q = Queue(w, blocks_per_item=g, block_threads=nt, stages=st,
                       flags=FLAG_ORDER_BY_LAYERS if ordered else 0)
             q.run(dt, dh, do)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

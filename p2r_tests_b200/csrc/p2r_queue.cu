@@ -98,23 +98,25 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
 }
 
 // ---------------------------------------------------------------- ordered variant
-// Each CTA (8 warps) takes a chunk of an item, floor(512 / bsize) blocks (at most 512 tracks), and
+// Each CTA (NW = 4 or 8 warps) takes a chunk of an item, floor(64 NW / bsize) blocks (at most
+// 64 NW tracks), and
 // orders the chunk's tracks by layer count (a stable counting sort in shared memory), so that the
 // 32 lanes of a warp run tracks of similar length and few lanes idle while a warp's longest track
-// runs. The ordered tracks form 16 groups of 32; warp w runs group w and then group 15 - w, one
+// runs. The ordered tracks form 2 NW groups of 32; warp w runs group w and then group 2NW-1-w, one
 // long and one short group, so the 8 warps finish the chunk at about the same time and the CTA
 // rarely holds a lone warp. A lane reads its own track's hits straight from the Matriplex rows
 // (the chunk's blocks are shared by the CTA's warps through L1), the next layer's hits loaded
 // while the current one computes; warps synchronise only at chunk boundaries. Per track the
 // arithmetic is the masked forward's, in the same order: bit-identical results.
-// nlayer <= 64 (the ordering keys), bsize <= 512.
-constexpr int kOrdThreads = 256;
-constexpr int kOrdWarps = kOrdThreads / 32;
-constexpr int kOrdTracks = 2 * kOrdThreads;  // tracks per chunk: two groups of 32 per warp
+// nlayer <= 64 (the ordering keys), bsize <= 64 NW.
 constexpr int kOrdMaxKeys = 65;
 
-template <int BS, int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
-__global__ void __launch_bounds__(kOrdThreads, 3) queue_ordered_kernel(QueueParams q) {
+// NW warps per CTA (4 or 8): chunks of 64 NW tracks; 24 resident warps per SM either way.
+template <int BS, int NW, bool CHI2, bool FP64DET, bool SQUASH>
+__global__ void __launch_bounds__(NW * 32, 24 / NW) queue_ordered_kernel(QueueParams q) {
+  constexpr int kOrdThreads = NW * 32;
+  constexpr int kOrdWarps = NW;
+  constexpr int kOrdTracks = 2 * kOrdThreads;
   __shared__ int s_order[kOrdTracks];
   __shared__ int s_wcount[kOrdWarps][kOrdMaxKeys];
   __shared__ int s_base[kOrdMaxKeys];
@@ -241,9 +243,10 @@ __global__ void __launch_bounds__(kOrdThreads, 3) queue_ordered_kernel(QueuePara
   }
 }
 
-template <int BS, int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
+template <int BS, int NW, bool CHI2, bool FP64DET, bool SQUASH>
 cudaError_t launch_queue_ordered_t(const QueueParams& q, int ctas_per_sm, cudaStream_t st) {
-  auto kern = queue_ordered_kernel<BS, STAGES, CHI2, FP64DET, SQUASH>;
+  constexpr int kOrdThreads = NW * 32;
+  auto kern = queue_ordered_kernel<BS, NW, CHI2, FP64DET, SQUASH>;
   int dev = 0, sms = 0, occ = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -256,13 +259,13 @@ cudaError_t launch_queue_ordered_t(const QueueParams& q, int ctas_per_sm, cudaSt
   return cudaGetLastError();
 }
 
-template <int STAGES, bool CHI2, bool FP64DET, bool SQUASH>
+template <int NW, bool CHI2, bool FP64DET, bool SQUASH>
 cudaError_t launch_queue_ordered_bs(const QueueParams& q, int ctas, cudaStream_t st) {
   switch (q.f.bsize) {
-    case 32: return launch_queue_ordered_t<32, STAGES, CHI2, FP64DET, SQUASH>(q, ctas, st);
-    case 64: return launch_queue_ordered_t<64, STAGES, CHI2, FP64DET, SQUASH>(q, ctas, st);
-    case 128: return launch_queue_ordered_t<128, STAGES, CHI2, FP64DET, SQUASH>(q, ctas, st);
-    default: return launch_queue_ordered_t<0, STAGES, CHI2, FP64DET, SQUASH>(q, ctas, st);
+    case 32: return launch_queue_ordered_t<32, NW, CHI2, FP64DET, SQUASH>(q, ctas, st);
+    case 64: return launch_queue_ordered_t<64, NW, CHI2, FP64DET, SQUASH>(q, ctas, st);
+    case 128: return launch_queue_ordered_t<128, NW, CHI2, FP64DET, SQUASH>(q, ctas, st);
+    default: return launch_queue_ordered_t<0, NW, CHI2, FP64DET, SQUASH>(q, ctas, st);
   }
 }
 
@@ -343,9 +346,14 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
   int rc = p2r_check_queue(q, who);
   if (rc) return rc;
   const bool ordered = (q->flags & P2R_FLAG_ORDER_BY_LAYERS) != 0;
-  if (ordered && (q->nlayer > kOrdMaxKeys - 1 || q->bsize > kOrdTracks))
-    return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_ORDER_BY_LAYERS needs nlayer <= %d and bsize <= %d", who,
-                          kOrdMaxKeys - 1, kOrdTracks);
+  // ordered launches: 8 warps per CTA (block_threads 0) or 4 (block_threads 128)
+  const int ord_warps = q->block_threads == 128 ? 4 : 8;
+  if (ordered && (q->nlayer > kOrdMaxKeys - 1 || q->bsize > 64 * ord_warps ||
+                  (q->block_threads != 0 && q->block_threads != 128)))
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED,
+                          "%s: P2R_FLAG_ORDER_BY_LAYERS needs nlayer <= %d, block_threads 0 (8 warps per CTA) or 128 "
+                          "(4 warps), and bsize <= 64 x warps per CTA",
+                          who, kOrdMaxKeys - 1);
   const QueueWs w = queue_ws(q->nevts);
   if (!workspace || ws_bytes < w.bytes)
     return p2r_set_errorf(P2R_ERR_WORKSPACE, "%s: workspace of %zu bytes needed", who, w.bytes);
@@ -410,16 +418,16 @@ int enqueue_queue(const p2r_queue* q, const void* trk_in, const void* hits, void
     if (qp.f.squash && !fp64) {
       e = cudaErrorNotSupported;  // rejected before launch in p2r_run_queue's checks
     } else if (ordered) {
-#define P2R_O(S, C, F, Q) launch_queue_ordered_bs<S, C, F, Q>(qp, c, st)
+#define P2R_O(W, C, F, Q) launch_queue_ordered_bs<W, C, F, Q>(qp, c, st)
       if (qp.f.squash)
-        e = stages == 2 ? (chi2 ? P2R_O(2, true, true, true) : P2R_O(2, false, true, true))
-                        : (chi2 ? P2R_O(4, true, true, true) : P2R_O(4, false, true, true));
-      else if (stages == 2)
-        e = chi2 ? (fp64 ? P2R_O(2, true, true, false) : P2R_O(2, true, false, false))
-                 : (fp64 ? P2R_O(2, false, true, false) : P2R_O(2, false, false, false));
-      else
+        e = ord_warps == 4 ? (chi2 ? P2R_O(4, true, true, true) : P2R_O(4, false, true, true))
+                           : (chi2 ? P2R_O(8, true, true, true) : P2R_O(8, false, true, true));
+      else if (ord_warps == 4)
         e = chi2 ? (fp64 ? P2R_O(4, true, true, false) : P2R_O(4, true, false, false))
                  : (fp64 ? P2R_O(4, false, true, false) : P2R_O(4, false, false, false));
+      else
+        e = chi2 ? (fp64 ? P2R_O(8, true, true, false) : P2R_O(8, true, false, false))
+                 : (fp64 ? P2R_O(8, false, true, false) : P2R_O(8, false, false, false));
 #undef P2R_O
     } else if (qp.f.squash) {
       e = stages == 2 ? (chi2 ? launch_queue_bs<2, true, true, true>(qp, threads, c, st)

@@ -143,9 +143,10 @@ def test_tune_queue_choice_reproduces_results(p2r, torch, tmp_path, monkeypatch)
     counts = p2r.lognormal_counts(8, median=120, sigma=0.8, lo=5, hi=600, seed=9)
     t = autotune.tune_queue(counts, bsizes=(32, 64), granularity=(1, 4), threads=(64, 128), stages=(4,), reps=1,
                             use_cache=False)
-    # per bsize: 2 granularities x 2 block shapes, plus 2 granularities with in-launch ordering
-    assert len(t["tried"]) == 2 * (2 * 2 + 2)
-    assert sum(1 for x in t["tried"] if x["order"]) == 4
+    # per bsize: 2 granularities x 2 block shapes, plus 2 granularities x 2 CTA sizes with
+    # in-launch ordering
+    assert len(t["tried"]) == 2 * (2 * 2 + 2 * 2)
+    assert sum(1 for x in t["tried"] if x["order"]) == 8
     assert t["ms"] == min(x["ms"] for x in t["tried"])
     assert all(x["p50_event_ms"] <= x["p99_event_ms"] for x in t["tried"])
     w = p2r.uneven_workload(counts, bsize=t["bsize"], nlayer_max=25)
@@ -153,7 +154,7 @@ def test_tune_queue_choice_reproduces_results(p2r, torch, tmp_path, monkeypatch)
     dh = torch.from_numpy(w["hit"].reshape(-1)).cuda()
     outs = []
     fl = p2r.FLAG_ORDER_BY_LAYERS if t["order"] else 0
-    for g, nt, f in ((t["blocks_per_item"], 0 if fl else t["block_threads"], fl), (1, 64, 0)):
+    for g, nt, f in ((t["blocks_per_item"], t["block_threads"], fl), (1, 64, 0)):
         o = torch.empty_like(dt)
         p2r.Queue(w, blocks_per_item=g, block_threads=nt, stages=t["stages"], flags=f).run(dt, dh, o)
         outs.append(bits(o.cpu().numpy()))

@@ -89,7 +89,7 @@ def small_batch(p2r):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("g,flags", [(1, 0), (4, 0), (16, 0), (4, "squash"), (1, "order"), (8, "order"), (20, "order"),
-                                     (8, "order+squash")])
+                                     (8, "order+squash"), (3, "order4"), (8, "order4")])
 def test_queue_matches_masked_forward(p2r, torch, small_batch, g, flags):
     """The persistent queue performs the masked fused forward's operations: bit-identical
     (also with phi wrapped after every update, and with each CTA's tracks ordered by layer
@@ -97,7 +97,7 @@ def test_queue_matches_masked_forward(p2r, torch, small_batch, g, flags):
     w = small_batch
     fl = (p2r.FLAG_SQUASH_PHI if "squash" in str(flags) else 0) | (p2r.FLAG_ORDER_BY_LAYERS if "order" in str(flags)
                                                                    else 0)
-    q = p2r.Queue(w, blocks_per_item=g, flags=fl)
+    q = p2r.Queue(w, blocks_per_item=g, flags=fl, block_threads=128 if "order4" in str(flags) else 0)
     t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
     out = torch.empty_like(t)
     q.run(t, h, out)
