@@ -2,8 +2,9 @@
 point is placed between two 4 KB guard regions filled with a sentinel bit pattern, and after the
 call the guards must be bit-for-bit unchanged. Shapes are odd on purpose: bsize 1 and 96 (the
 plain-load path), bsize 32 with ragged per-track layer counts, the restart loop, the per-layer
-calls, the host-buffer pipeline, the persistent queue, both adjoint paths with per-event
-gradients, and the device-side generator."""
+calls, the host-buffer pipeline, the persistent queue (plain and ordered by layer count, bsize 32,
+64 and 96), the grid and persistent adjoint paths with per-event gradients, the 3x3 gain routines
+and the device-side generator."""
 import ctypes
 
 import numpy as np
@@ -93,10 +94,12 @@ def test_per_layer_calls_and_host_pipeline_stay_in_bounds(p2r, torch):
     assert d_t.intact() and d_h.intact() and d_o.intact()
 
 
-def test_queue_writes_stay_in_bounds(p2r, torch):
-    w = p2r.uneven_workload(p2r.lognormal_counts(7, median=60, sigma=1.0, lo=1, hi=400, seed=2), bsize=32,
+@pytest.mark.parametrize("bs,ordered,threads", [(32, False, 64), (32, True, 0), (64, True, 128), (96, True, 0)])
+def test_queue_writes_stay_in_bounds(p2r, torch, bs, ordered, threads):
+    w = p2r.uneven_workload(p2r.lognormal_counts(7, median=60, sigma=1.0, lo=1, hi=400, seed=2), bsize=bs,
                             nlayer_max=25)
-    q = p2r.Queue(w, blocks_per_item=2, block_threads=64)
+    q = p2r.Queue(w, blocks_per_item=3 if ordered else 2, block_threads=threads,
+                  flags=p2r.FLAG_ORDER_BY_LAYERS if ordered else 0)
     ws = Guarded(torch, q.ws.numel(), torch.uint8)
     done = Guarded(torch, q.done_ns.numel(), q.done_ns.dtype)
     start = Guarded(torch, q.start_ns.numel(), q.start_ns.dtype)
@@ -107,6 +110,37 @@ def test_queue_writes_stay_in_bounds(p2r, torch):
     chi2 = Guarded(torch, trk.numel() // 28, torch.float32)
     q.run(trk, hit, out.t, chi2=chi2.t)
     assert all(g.intact() for g in (ws, done, start, out, chi2))
+    assert q.error_bits() == 0
+
+
+@pytest.mark.parametrize("ordered", [False, True])
+def test_queue_adjoint_writes_stay_in_bounds(p2r, torch, ordered):
+    w = p2r.uneven_workload(p2r.lognormal_counts(6, median=70, sigma=1.0, lo=1, hi=300, seed=4), bsize=32,
+                            nlayer_max=21, lay_lo=3, lay_hi=21)
+    q = p2r.Queue(w, blocks_per_item=2, flags=p2r.FLAG_ORDER_BY_LAYERS if ordered else 0)
+    trk = torch.from_numpy(w["trk"].reshape(-1)).cuda()
+    hit = torch.from_numpy(w["hit"].reshape(-1)).cuda()
+    ntr, nl, ne = trk.numel() // 28, w["nlayer"], q.nevts
+    f32, f64 = torch.float32, torch.float64
+    g = {"trk_out": Guarded(torch, trk.numel(), f32), "chi2": Guarded(torch, ntr, f32),
+         "grad_trk_in": Guarded(torch, trk.numel(), f32), "grad_hits": Guarded(torch, hit.numel(), f32),
+         "grad_dr": Guarded(torch, nl, f64), "grad_bz": Guarded(torch, 1, f64),
+         "grad_dr_event": Guarded(torch, ne * nl, f64), "grad_bz_event": Guarded(torch, ne, f64),
+         "workspace": Guarded(torch, q.adjoint_workspace_size(), torch.uint8)}
+    out = {k: v.t for k, v in g.items()}
+    q.run_adjoint(trk, hit, dr=torch.zeros(nl, device="cuda"), grad_chi2=torch.ones(ntr, device="cuda"), out=out)
+    bad = [k for k, v in g.items() if not v.intact()]
+    assert not bad, bad
+    assert q.error_bits() == 0
+
+
+def test_gain3_writes_stay_in_bounds(p2r, torch):
+    cfg, trk, hit = inputs(p2r, torch, 96, 2, 3, 11)
+    inv = Guarded(torch, cfg.nblocks * 9 * 96, torch.float32)
+    gain = Guarded(torch, cfg.nblocks * 18 * 96, torch.float32)
+    p2r.KalmanGainInv(cfg, trk, hit, 10, inv.t)
+    p2r.KalmanGain(cfg, trk, inv.t, gain.t)
+    assert inv.intact() and gain.intact()
 
 
 @pytest.mark.parametrize("tape,ckpt", [(True, 1), (True, 5), (False, 5)])
