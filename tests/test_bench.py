@@ -19,7 +19,7 @@ def bench():
 
 
 def test_constants_from_committed_profiles(bench):
-    assert bench.traffic_from_profiles("chained") == pytest.approx(8.40e8)
+    assert bench.traffic_from_profiles("chained") == pytest.approx(8.45e8)
     assert bench.traffic_from_profiles("restart") == pytest.approx(1.42e8)
     assert bench.fp64_flop_per_update() == pytest.approx(3698)
 
