@@ -711,6 +711,17 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         fms_sorted = f0.elapsed_time(f1) / args.calib_steps
+        # the masked forward with each CTA's tracks ordered by layer count inside the launch
+        c4f = dataclasses.replace(c4, flags=c4.flags | p2r.FLAG_ORDER_BY_LAYERS)
+        for _ in range(2):
+            p2r.forward(c4f, t4, h4, o4, dr=dr4, nlay_lane=nl4, stream=stream)
+        torch.cuda.synchronize()
+        f0.record(stream)
+        for _ in range(args.calib_steps):
+            p2r.forward(c4f, t4, h4, o4, dr=dr4, nlay_lane=nl4, stream=stream)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fms_ordered = f0.elapsed_time(f1) / args.calib_steps
         del o4
         gc4 = torch.ones(c4.ntracks, dtype=torch.float32, device=dev)
         out4 = {"grad_trk_in": None, "grad_hits": None}
@@ -814,7 +825,11 @@ def main():
                  "forward": {"ms_per_step": fms, "updates_per_s": upd4 / (fms / 1e3),
                              "api": "p2r_forward_masked (fused, per-track layer counts)",
                              "sorted_by_layer_count": {"ms_per_step": fms_sorted,
-                                                       "updates_per_s": upd4 / (fms_sorted / 1e3)}},
+                                                       "updates_per_s": upd4 / (fms_sorted / 1e3)},
+                             "ordered_in_launch": {"ms_per_step": fms_ordered,
+                                                   "updates_per_s": upd4 / (fms_ordered / 1e3),
+                                                   "how": "P2R_FLAG_ORDER_BY_LAYERS: each CTA orders its "
+                                                          "chunk of 512 tracks by layer count"}},
                  "forward_adjoint": {
                      "ms_per_step": qadj["ordered_by_layers"]["ms_per_step"],
                      "ratio_vs_forward": qadj["ordered_by_layers"]["ratio_vs_forward"],

@@ -62,15 +62,17 @@ typedef enum p2r_mode { P2R_MODE_RESTART = 0, P2R_MODE_CHAINED = 1 } p2r_mode;
 #define P2R_FLAG_SQUASH_PHI 0x8u /* wrap phi into [-pi, pi] after every update: the step the reference
                                     leaves commented out (squashPhiMPlex, TBB:635); forward entry points,
                                     with the FP64 determinant (not with P2R_FLAG_FP32_DET) */
-#define P2R_FLAG_ORDER_BY_LAYERS 0x10u /* with per-track layer counts: inside the launch, order each
-                                    event's tracks by layer count (longest first, ties in track order),
-                                    so a warp's lanes run tracks of similar length: within windows of
-                                    512 tracks (whole blocks) for p2r_forward_backward and the forward
-                                    queue, over whole events for the queue adjoint. Outputs stay at each track's own position and every
-                                    track's result is the same arithmetic; shared gradient sums are
-                                    added in the new grouping. p2r_forward_backward (cfg.flags; uses
-                                    4 bytes of workspace per track), the queue adjoint and the forward
-                                    queue (p2r_queue.flags; nlayer <= 64, bsize <= 256) */
+#define P2R_FLAG_ORDER_BY_LAYERS 0x10u /* with per-track layer counts: inside the launch, order the
+                                    tracks by layer count (longest first, ties in track order) so a
+                                    warp's lanes run tracks of similar length; outputs stay at each
+                                    track's own position and every track's result is the same
+                                    arithmetic (shared gradient sums are added in the new grouping).
+                                    p2r_forward_masked (cfg.flags): within each CTA's chunk of 256 or
+                                    512 tracks (FP64 determinant, nlayer <= 64, bsize <= 512); the
+                                    forward queue (p2r_queue.flags): the same per chunk of an item;
+                                    p2r_forward_backward (cfg.flags): within windows of 512 tracks of
+                                    each event, 4 bytes of workspace per track; the queue adjoint
+                                    (p2r_queue.flags): over whole events */
 
 typedef struct p2r_config {
   int32_t bsize;         /* Matriplex lanes per block (TBB:15-17); >= 1 */

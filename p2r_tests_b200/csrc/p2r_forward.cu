@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include "p2r_fwd.cuh"
+#include "p2r_fwd_ordered.cuh"
 #include "p2r_internal.h"
 
 namespace p2r {
@@ -144,10 +145,20 @@ static int forward_impl(const p2r_config* cfg, const void* trk_in, const void* h
   const bool fp64det = !(cfg->flags & P2R_FLAG_FP32_DET);
   if (p.squash && !fp64det)
     return p2r_set_errorf(P2R_ERR_UNSUPPORTED, "%s: P2R_FLAG_SQUASH_PHI is built with the FP64 determinant only", who);
+  // ordering by layer count matters only with per-track layer counts (chained)
+  const bool ordered = nlay && (cfg->flags & P2R_FLAG_ORDER_BY_LAYERS);
+  if (ordered && (!fp64det || cfg->nlayer > kOrdMaxKeys - 1 ||
+                  cfg->bsize > (threads == 128 ? 2 * 128 : 2 * 256) || cfg->bsize % 32 != 0))
+    return p2r_set_errorf(P2R_ERR_UNSUPPORTED,
+                          "%s: P2R_FLAG_ORDER_BY_LAYERS needs the FP64 determinant, nlayer <= %d, a bsize that is a "
+                          "multiple of 32 and at most 2 x the CTA size (block_threads 128: 4 warps, else 8)",
+                          who, kOrdMaxKeys - 1);
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
   if (cfg->mode == P2R_MODE_RESTART)
     e = launch_restart(p, fp64det, threads, stages, st);
+  else if (ordered)
+    e = launch_ordered(p, fp64det, threads, st);
   else if (nlay)
     e = launch_masked(p, staged, fp64det, threads, stages, st);
   else

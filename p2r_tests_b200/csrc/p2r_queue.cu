@@ -18,6 +18,7 @@
 #include <new>
 
 #include "p2r_fwd.cuh"
+#include "p2r_fwd_ordered.cuh"
 #include "p2r_internal.h"
 #include "p2r_queue_check.cuh"
 
@@ -98,38 +99,17 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
 }
 
 // ---------------------------------------------------------------- ordered variant
-// Each CTA (NW = 4 or 8 warps) takes a chunk of an item, floor(64 NW / bsize) blocks (at most
-// 64 NW tracks), and
-// orders the chunk's tracks by layer count (a stable counting sort in shared memory), so that the
-// 32 lanes of a warp run tracks of similar length and few lanes idle while a warp's longest track
-// runs. The ordered tracks form 2 NW groups of 32; warp w runs group w and then group 2NW-1-w, one
-// long and one short group, so the 8 warps finish the chunk at about the same time and the CTA
-// rarely holds a lone warp. A lane reads its own track's hits straight from the Matriplex rows
-// (the chunk's blocks are shared by the CTA's warps through L1), the next layer's hits loaded
-// while the current one computes; warps synchronise only at chunk boundaries. Per track the
-// arithmetic is the masked forward's, in the same order: bit-identical results.
-// nlayer <= 64 (the ordering keys), bsize <= 64 NW.
-constexpr int kOrdMaxKeys = 65;
-
-// NW warps per CTA (4 or 8): chunks of 64 NW tracks; 24 resident warps per SM either way.
+// The same queue with each item's blocks run in chunks whose tracks are ordered by layer count
+// (P2R_FLAG_ORDER_BY_LAYERS; ordered_chunk in p2r_fwd_ordered.cuh).
 template <int BS, int NW, bool CHI2, bool FP64DET, bool SQUASH>
 __global__ void __launch_bounds__(NW * 32, 24 / NW) queue_ordered_kernel(QueueParams q) {
-  constexpr int kOrdThreads = NW * 32;
-  constexpr int kOrdWarps = NW;
-  constexpr int kOrdTracks = 2 * kOrdThreads;
-  __shared__ int s_order[kOrdTracks];
-  __shared__ int s_wcount[kOrdWarps][kOrdMaxKeys];
-  __shared__ int s_base[kOrdMaxKeys];
-  __shared__ int s_cnt[2][kOrdMaxKeys];
+  __shared__ OrdSmem<NW> sm;
   __shared__ long long s_item;
   const FwdParams& p = q.f;
   const int bs = BS > 0 ? BS : p.bsize;
   const int spb = bs / 32;
-  const int cb = kOrdTracks / bs;  // blocks per chunk
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nkeys = p.nlayer + 1;
-  const unsigned lt = (1u << lane) - 1u;
-  const long long lstride = (long long)kHitWords * bs;
+  const int cb = ordered_chunk_blocks<NW>(bs);
+  const int tid = threadIdx.x;
   if (tid == 0 && q.t_start) atomicMin(q.t_start, globaltimer_ns());
   for (;;) {
     if (tid == 0) s_item = atomicAdd(q.counter, 1);
@@ -144,96 +124,8 @@ __global__ void __launch_bounds__(NW * 32, 24 / NW) queue_ordered_kernel(QueuePa
       continue;
     }
     for (int c0 = 0; c0 < qi.nblk; c0 += cb) {
-      const long long b0 = qi.block0 + c0;
       const int nblk = min(cb, qi.nblk - c0);
-      const int ntrk = nblk * bs;
-      // ---- order the chunk's tracks: stable counting sort on key = nlayer - layers, over two
-      // passes of 256 tracks (track t = pass * 256 + tid); a track's rank among equal keys comes
-      // from its warp (__match_any_sync) and the warps before it, pass 1 after all of pass 0
-      int keyv[2], rankv[2];
-#pragma unroll
-      for (int pass = 0; pass < 2; ++pass) {
-        const int t = pass * kOrdThreads + tid;
-        int key = -1;
-        if (t < ntrk) {
-          const int v = p.nlay[(b0 + t / bs) * bs + t % bs];
-          key = p.nlayer - min(p.nlayer, max(0, v));
-        }
-        const unsigned same = __match_any_sync(0xffffffffu, key);
-        int r = __popc(same & lt);
-        for (int j = lane; j < nkeys; j += 32) s_wcount[warp][j] = 0;
-        __syncwarp();
-        if (key >= 0 && r == 0) s_wcount[warp][key] = __popc(same);
-        __syncthreads();
-        if (key >= 0)
-          for (int w = 0; w < warp; ++w) r += s_wcount[w][key];
-        if (tid < nkeys) {
-          int tot = 0;
-          for (int w = 0; w < kOrdWarps; ++w) tot += s_wcount[w][tid];
-          s_cnt[pass][tid] = tot;
-        }
-        keyv[pass] = key;
-        rankv[pass] = r;
-        __syncthreads();  // s_wcount is reused by the next pass
-      }
-      if (tid == 0) {  // first position of each key
-        int run = 0;
-        for (int k = 0; k < nkeys; ++k) {
-          s_base[k] = run;
-          run += s_cnt[0][k] + s_cnt[1][k];
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int pass = 0; pass < 2; ++pass) {
-        const int key = keyv[pass];
-        if (key >= 0) s_order[s_base[key] + (pass ? s_cnt[0][key] : 0) + rankv[pass]] = pass * kOrdThreads + tid;
-      }
-      __syncthreads();
-      // ---- two ordered groups per warp: group w (long tracks), then group 15 - w (short)
-      for (int half = 0; half < 2; ++half) {
-        const int grp = half == 0 ? warp : 2 * kOrdWarps - 1 - warp;
-        const int pos = grp * 32 + lane;
-        const bool mine = pos < ntrk;
-        const int li = mine ? s_order[pos] : 0;
-        const int jb = li / bs, it = li - jb * bs;
-        const long long b = b0 + jb;
-        float par[6], cov[21];
-        int qq = 1, nl = 0;
-        if (mine) {
-          load_track(p.trk_in + b * (long long)(kTrkWords * bs), bs, it, par, cov, qq);
-          nl = min(p.nlayer, max(0, p.nlay[b * bs + it]));
-        }
-        const float k = (float)qq * p.kfact;
-        const float kinv = 1.f / k;
-        float chi2 = 0.f;
-        const float* hb = p.hits + b * (long long)p.nlayer * lstride + it;
-        float hn[9];
-        if (nl > 0) {
-#pragma unroll
-          for (int i = 0; i < 9; ++i) hn[i] = __ldg(hb + i * bs);
-        }
-        for (int l = 0; l < nl; ++l) {
-          float hp[3], hc[6];
-#pragma unroll
-          for (int i = 0; i < 3; ++i) hp[i] = hn[i];
-#pragma unroll
-          for (int i = 0; i < 6; ++i) hc[i] = hn[3 + i];
-          if (l + 1 < nl) {  // the next layer's hit, in flight while this layer computes
-#pragma unroll
-            for (int i = 0; i < 9; ++i) hn[i] = __ldg(hb + (l + 1) * lstride + i * bs);
-          }
-          const float rh = hipo(hp[0], hp[1]);
-          propagate_to_r(par, cov, k, kinv, rh, par, cov);
-          chi2 += kalman_update<FP64DET, CHI2>(par, cov, hp, hc, rh);
-          if (SQUASH) par[4] = squash_phi(par[4]);
-        }
-        if (mine) {
-          store_track(p.trk_out + b * (long long)(kTrkWords * bs), bs, it, par, cov, qq);
-          if (CHI2) p.chi2[b * bs + it] = chi2;
-        }
-      }
-      __syncthreads();  // the order is reused by the next chunk
+      ordered_chunk<BS, NW, CHI2, false, FP64DET, SQUASH>(p, qi.block0 + c0, nblk, sm);
       if (tid == 0) {
         __threadfence();
         if (atomicSub(&q.ev_remaining[qi.event], nblk * spb) == nblk * spb && q.ev_done)

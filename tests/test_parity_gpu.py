@@ -576,3 +576,29 @@ def test_calibration_full_size_sampled_against_fp64(p2r, oracle, torch):
     for what, a, b in (("param", qt[0], qr[0]), ("cov", qt[1], qr[1])):
         for q, x, y in zip(parity.ACC_QUANTILES, a, b):
             assert x <= parity.ACC_FACTOR * y + 1e-7, f"{what} q{q}: GPU {x:.3e} vs reference {y:.3e}"
+
+
+@pytest.mark.parametrize("bs,threads,opts", [(32, 0, ""), (32, 128, "chi2+dr"), (64, 0, "chi2+dr+squash"),
+                                              (96, 128, "dr"), (32, 0, "chi2+dr+40")])
+def test_masked_forward_ordered_by_layers_identical(p2r, torch, bs, threads, opts):
+    """P2R_FLAG_ORDER_BY_LAYERS on the masked fused forward: each CTA orders its chunk's tracks by
+    layer count; every output (tracks, chi2) is bit-identical to the unordered launch's."""
+    nlayer = 40 if "40" in opts else 25
+    cfg, trk, hit = helix(p2r, 3, 700 // bs + 1, nlayer=nlayer, bs=bs)
+    rng = np.random.default_rng(bs + threads)
+    nl = rng.integers(0, nlayer + 1, cfg.ntracks).astype(np.int32)
+    nl[:bs] = nlayer  # a block at full length, and one with every lane empty
+    nl[bs:2 * bs] = 0
+    dr = rng.uniform(-0.01, 0.01, nlayer).astype(np.float32) if "dr" in opts else None
+    fl = p2r.FLAG_SQUASH_PHI if "squash" in opts else 0
+    outs = []
+    for order in (False, True):
+        c = p2r.Config(**{**cfg.__dict__, "block_threads": threads,
+                          "flags": fl | (p2r.FLAG_ORDER_BY_LAYERS if order else 0)})
+        outs.append(gpu_forward(p2r, torch, c, trk, hit, chi2="chi2" in opts, dr=dr, nlay_lane=nl))
+    if "chi2" in opts:
+        (a, ca), (b, cb) = outs
+        assert np.array_equal(ca.view(np.uint32), cb.view(np.uint32))
+    else:
+        a, b = outs
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
