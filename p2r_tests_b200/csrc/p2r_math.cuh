@@ -84,9 +84,6 @@ __device__ __forceinline__ float fsqrt(float x) { return __fsqrt_rn(x); }
 // sqrt(x^2 + y^2)
 __device__ __forceinline__ float hipo(float x, float y) { return fsqrt(ffma(x, x, fmul(y, y))); }
 
-// 1 / (e0 e2 - e1^2) with the determinant and its reciprocal in double, rounded once to float
-// (TBB:457-459). The float products are exact in double, so only the difference and the
-// reciprocal round.
 // The inverse of the symmetric 2x2 [[e0, e1], [e1, e2]] with the determinant, its reciprocal
 // and the three products in double, each entry rounded to float once (TBB:457-463 takes the
 // determinant and its reciprocal in double). Rounding 1/det to float before the products, as
