@@ -263,3 +263,50 @@ def test_queue_skips_and_reports_malformed_items(p2r, torch, small_batch):
     q.d_off.copy_(d_off)
     q.run(t, h, torch.empty_like(t))
     assert q.error_bits() == 0
+
+
+@pytest.mark.gpu
+def test_uneven_batch_full_size(p2r, oracle, torch):
+    """The 1000-event uneven batch at full size (log-normal tracks per event, median 2000,
+    10-25 layers per track; 2.9e6 tracks, 5.0e7 updates) through the launch the benchmark
+    times: the ordered persistent queue (bsize 32, 8 blocks per item, 4-warp CTAs) replayed from
+    its CUDA graph. Size-independent properties: every track bit-identical to the masked fused
+    forward over the same arrays, padding lanes returned unchanged, no queue error; and on the
+    first 40 events (7.4e4 tracks) accuracy parity with the reference's own masked chain
+    against the FP64 oracle."""
+    from oracle.oracle import RefTBB, ref_available
+    w = p2r.uneven_workload(p2r.lognormal_counts(1000, median=2000, sigma=1.0, lo=50, hi=20000, seed=7), bsize=32,
+                            nlayer_max=25)
+    q = p2r.Queue(w, blocks_per_item=8, block_threads=128, flags=p2r.FLAG_ORDER_BY_LAYERS)
+    t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
+    out = torch.full_like(t, float("nan"))
+    q.capture(t, h, out)
+    q.replay()
+    q.replay()
+    torch.cuda.synchronize()
+    assert q.error_bits() == 0
+    q.release()
+    ref = torch.empty_like(t)
+    cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"])
+    p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    del t, h, out
+    assert np.array_equal(got.view(np.uint32), ref.cpu().numpy().view(np.uint32))
+    del ref
+    live = w["nlay_lane"] > 0
+    lanes = lambda a: a.reshape(-1, 28, 32).transpose(0, 2, 1).reshape(-1, 28)
+    assert np.array_equal(lanes(got)[~live].view(np.uint32), lanes(w["trk"])[~live].view(np.uint32))
+    if not ref_available(32, "kf"):
+        pytest.skip("reference build not present")
+    nb = int(w["event_block_offset"][40])
+    trk, hit = w["trk"].reshape(-1)[:nb * 28 * 32], w["hit"].reshape(-1)[:nb * w["nlayer"] * 9 * 32]
+    nl = w["nlay_lane"][:nb * 32]
+    r = RefTBB(32, "kf")
+    r.set_bz(w["bz"])
+    want = r.run_masked(trk, hit, w["nlayer"], nl)
+    f64 = oracle.run(trk, hit, 32, w["nlayer"], 1, w["bz"], "f64", nlay_lane=nl)
+    sl = nl > 0
+    one = lambda a: lanes(a)[sl].reshape(-1, 1, 28).transpose(0, 2, 1).reshape(-1)
+    parity.assert_accuracy_parity(one(got[:nb * 28 * 32]), one(want), f64["par"][sl], f64["cov"][sl],
+                                  f64["prior"][sl], 1, "uneven batch, first 40 events, vs reference (masked)")
