@@ -3,7 +3,7 @@
 Reference gradient: torch autograd in FP64 over oracle/p2r_torch.py (pinned to the C
 oracle and to central finite differences in tests/test_adjoint_cpu.py). Tolerance: each
 gradient within 1e-3 relative of the FP64 reference, relative to max(|g|, 1e-3 * the
-largest |g| of that gradient group) so components that are zero to rounding are judged
+largest |g| of that gradient group) so components that are zero to rounding are measured
 against the group's scale. The default adjoint runs in FP64; the FP32 mode
 (P2R_FLAG_ADJ_FP32) is held to its measured accuracy instead.
 """
