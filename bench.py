@@ -829,7 +829,7 @@ def main():
                              "ordered_in_launch": {"ms_per_step": fms_ordered,
                                                    "updates_per_s": upd4 / (fms_ordered / 1e3),
                                                    "how": "P2R_FLAG_ORDER_BY_LAYERS: each CTA orders its "
-                                                          "chunk of 512 tracks by layer count"}},
+                                                          "chunk of 256 tracks by layer count"}},
                  "forward_adjoint": {
                      "ms_per_step": qadj["ordered_by_layers"]["ms_per_step"],
                      "ratio_vs_forward": qadj["ordered_by_layers"]["ratio_vs_forward"],

@@ -6,7 +6,7 @@
 namespace p2r {
 
 template <int BS, int NW, bool CHI2, bool DR, bool SQUASH>
-__global__ void __launch_bounds__(NW * 32, 24 / NW) fwd_ordered_kernel(FwdParams p) {
+__global__ void __launch_bounds__(NW * 32, kOrdWarpsPerSm / NW) fwd_ordered_kernel(FwdParams p) {
   __shared__ OrdSmem<NW> sm;
   const int bs = BS > 0 ? BS : p.bsize;
   const int cb = ordered_chunk_blocks<NW>(bs);

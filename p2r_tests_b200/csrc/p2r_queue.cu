@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(128) queue_kernel(QueueParams q) {
 // The same queue with each item's blocks run in chunks whose tracks are ordered by layer count
 // (P2R_FLAG_ORDER_BY_LAYERS; ordered_chunk in p2r_fwd_ordered.cuh).
 template <int BS, int NW, bool CHI2, bool FP64DET, bool SQUASH>
-__global__ void __launch_bounds__(NW * 32, 24 / NW) queue_ordered_kernel(QueueParams q) {
+__global__ void __launch_bounds__(NW * 32, kOrdWarpsPerSm / NW) queue_ordered_kernel(QueueParams q) {
   __shared__ OrdSmem<NW> sm;
   __shared__ long long s_item;
   const FwdParams& p = q.f;
