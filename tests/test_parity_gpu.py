@@ -541,7 +541,9 @@ def test_calibration_full_size_sampled_against_fp64(p2r, oracle, torch):
     r = 4..110 cm, 20-40 layers per track, generated on the device; 15.5 GB of inputs), masked
     fused forward; the FP64 oracle's error sampled on 1 % of the tracks (every 100th track block)
     and compared with the reference's own masked CPU run on the same tracks: the GPU is at least as
-    accurate at every error quantile and keeps every sampled track finite that the reference does."""
+    accurate at every error quantile and keeps every sampled track finite that the reference does.
+    The launch with the tracks ordered by layer count inside it (P2R_FLAG_ORDER_BY_LAYERS) gives
+    every track bit for bit the same output."""
     from oracle.oracle import RefTBB, ref_available
     if not ref_available(32, "kf"):
         pytest.skip("reference build not present")
@@ -552,7 +554,13 @@ def test_calibration_full_size_sampled_against_fp64(p2r, oracle, torch):
                          generator=torch.Generator("cuda").manual_seed(4))
     out = torch.empty_like(trk)
     p2r.forward(cfg, trk, hit, out, nlay_lane=nlay)
+    # the same forward with each CTA's tracks ordered by layer count inside the launch: bit-identical
+    ordered = torch.full_like(trk, float("nan"))
+    p2r.forward(p2r.Config(**{**cfg.__dict__, "flags": cfg.flags | p2r.FLAG_ORDER_BY_LAYERS}), trk, hit, ordered,
+                nlay_lane=nlay)
     torch.cuda.synchronize()
+    assert torch.equal(ordered.view(torch.int32), out.view(torch.int32))
+    del ordered
     blocks = torch.arange(0, cfg.nblocks, 100, device="cuda")
     t_s = trk.view(cfg.nblocks, -1)[blocks].cpu().numpy().reshape(-1)
     h_s = hit.view(cfg.nblocks, -1)[blocks].cpu().numpy().reshape(-1)
