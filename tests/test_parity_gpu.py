@@ -393,9 +393,12 @@ def test_count_nonfinite(p2r, torch):
 
 
 @pytest.mark.slow
-def test_full_size_chained_sample_vs_reference(p2r, oracle, torch):
-    """9600 tracks x 100 events x 20 layers on the GPU; 300 blocks checked against the reference."""
+@pytest.mark.parametrize("mode", list(MODES))
+def test_full_size_sample_vs_reference(p2r, oracle, torch, mode):
+    """9600 tracks x 100 events x 20 layers on the GPU, chained and restart; 300 blocks checked
+    against the reference: restart element-wise at the stated bar, chained by accuracy parity."""
     cfg, trk, hit = helix(p2r, 100, 300)
+    cfg.mode = MODES[mode]
     out = gpu_forward(p2r, torch, cfg, trk, hit)
     assert np.isfinite(parity.unpack(out[: 600 * 28 * 32], 32)[0]).all()
     dt = dev(torch, out)
@@ -407,10 +410,13 @@ def test_full_size_chained_sample_vs_reference(p2r, oracle, torch):
     sel = np.random.default_rng(3).choice(cfg.nblocks, 300, replace=False)
     t_s = np.ascontiguousarray(trk[sel])
     h_s = np.ascontiguousarray(hit.reshape(cfg.nblocks, cfg.nlayer, 9, 32)[sel])
-    want = ref.run(t_s, h_s, 1, 300, cfg.nlayer, chained=True)
-    got = out.reshape(cfg.nblocks, 28, 32)[sel]
-    f64 = oracle.run(t_s, h_s, 32, cfg.nlayer, 1, cfg.bz, "f64")
-    parity.assert_accuracy_parity(got, want, f64["par"], f64["cov"], f64["prior"], 32, "full size sample")
+    want = ref.run(t_s, h_s, 1, 300, cfg.nlayer, chained=bool(MODES[mode]))
+    got = np.ascontiguousarray(out.reshape(cfg.nblocks, 28, 32)[sel])
+    f64 = oracle.run(t_s, h_s, 32, cfg.nlayer, MODES[mode], cfg.bz, "f64")
+    if mode == "restart":
+        parity.assert_elementwise(got, want, f64["prior"], 32, "full size sample, restart")
+    else:
+        parity.assert_accuracy_parity(got, want, f64["par"], f64["cov"], f64["prior"], 32, "full size sample")
 
 
 def test_arrays_beyond_32_bit_offsets(p2r, torch):
