@@ -88,25 +88,32 @@ def small_batch(p2r):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("g,flags", [(1, 0), (4, 0), (16, 0), (4, "squash"), (1, "order"), (8, "order"), (20, "order"),
-                                     (8, "order+squash"), (3, "order4"), (8, "order4")])
+@pytest.mark.parametrize("g,flags", [(1, 0), (4, 0), (16, 0), (4, "squash"), (4, "chi2"), (1, "order"), (8, "order"),
+                                     (20, "order"), (8, "order+squash"), (8, "order+chi2"), (3, "order4"),
+                                     (8, "order4+chi2")])
 def test_queue_matches_masked_forward(p2r, torch, small_batch, g, flags):
     """The persistent queue performs the masked fused forward's operations: bit-identical
-    (also with phi wrapped after every update, and with each CTA's tracks ordered by layer
-    count: P2R_FLAG_ORDER_BY_LAYERS)."""
+    tracks and chi2 (also with phi wrapped after every update, and with each CTA's tracks ordered
+    by layer count: P2R_FLAG_ORDER_BY_LAYERS)."""
     w = small_batch
     fl = (p2r.FLAG_SQUASH_PHI if "squash" in str(flags) else 0) | (p2r.FLAG_ORDER_BY_LAYERS if "order" in str(flags)
                                                                    else 0)
     q = p2r.Queue(w, blocks_per_item=g, flags=fl, block_threads=128 if "order4" in str(flags) else 0)
     t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
     out = torch.empty_like(t)
-    q.run(t, h, out)
+    with_chi2 = "chi2" in str(flags)
+    ntrk = w["nblocks"] * w["bsize"]
+    c2 = torch.full((ntrk,), float("nan"), device="cuda") if with_chi2 else None
+    q.run(t, h, out, c2)
     cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"],
                      flags=fl & ~p2r.FLAG_ORDER_BY_LAYERS)
     ref = torch.empty_like(t)
-    p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
+    rc2 = torch.zeros(ntrk, device="cuda") if with_chi2 else None
+    p2r.forward(cfg, t, h, ref, chi2=rc2, nlay_lane=dev(torch, w["nlay_lane"]))
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32)), (g, flags)
+    if with_chi2:
+        assert np.array_equal(c2.cpu().numpy().view(np.uint32), rc2.cpu().numpy().view(np.uint32)), (g, flags)
     lat = q.event_latency_ns()
     assert (lat > 0).all() and (lat < 10_000_000_000).all()
 
@@ -270,8 +277,8 @@ def test_uneven_batch_full_size(p2r, oracle, torch):
     """The 1000-event uneven batch at full size (log-normal tracks per event, median 2000,
     10-25 layers per track; 2.9e6 tracks, 5.0e7 updates) through the launch the benchmark
     times: the ordered persistent queue (bsize 32, 8 blocks per item, 4-warp CTAs) replayed from
-    its CUDA graph. Size-independent properties: every track bit-identical to the masked fused
-    forward over the same arrays, padding lanes returned unchanged, no queue error; and on the
+    its CUDA graph. Size-independent properties: every track and chi2 bit-identical to the masked
+    fused forward over the same arrays, padding lanes returned unchanged, no queue error; and on the
     first 40 events (7.4e4 tracks) accuracy parity with the reference's own masked chain
     against the FP64 oracle."""
     from oracle.oracle import RefTBB, ref_available
@@ -280,19 +287,23 @@ def test_uneven_batch_full_size(p2r, oracle, torch):
     q = p2r.Queue(w, blocks_per_item=8, block_threads=128, flags=p2r.FLAG_ORDER_BY_LAYERS)
     t, h = dev(torch, w["trk"]), dev(torch, w["hit"])
     out = torch.full_like(t, float("nan"))
-    q.capture(t, h, out)
+    ntrk = w["nblocks"] * w["bsize"]
+    c2 = torch.full((ntrk,), float("nan"), device="cuda")
+    q.capture(t, h, out, c2)
     q.replay()
     q.replay()
     torch.cuda.synchronize()
     assert q.error_bits() == 0
     q.release()
     ref = torch.empty_like(t)
+    rc2 = torch.zeros(ntrk, device="cuda")
     cfg = p2r.Config(bsize=32, nlayer=w["nlayer"], nevts=1, nb=w["nblocks"], bz=w["bz"])
-    p2r.forward(cfg, t, h, ref, nlay_lane=dev(torch, w["nlay_lane"]))
+    p2r.forward(cfg, t, h, ref, chi2=rc2, nlay_lane=dev(torch, w["nlay_lane"]))
     torch.cuda.synchronize()
     got = out.cpu().numpy()
     del t, h, out
     assert np.array_equal(got.view(np.uint32), ref.cpu().numpy().view(np.uint32))
+    assert np.array_equal(c2.cpu().numpy().view(np.uint32), rc2.cpu().numpy().view(np.uint32))
     del ref
     live = w["nlay_lane"] > 0
     lanes = lambda a: a.reshape(-1, 28, 32).transpose(0, 2, 1).reshape(-1, 28)
